@@ -1,0 +1,142 @@
+/*
+ * ising_b200.h — C ABI of the B200 (sm_100a) backend for pyising's sweep hot path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status (ISING_OK = 0).  Every call
+ * that fails leaves a message readable with ising_last_error() (thread-local).  A handle
+ * belongs to one host thread at a time and issues all its work on one CUDA stream; the library
+ * owns all device memory it allocates and never keeps a host pointer after a call returns.
+ *
+ * The reference interface each entry point replaces is cited as file:line inside the pyising
+ * project (github.com/walidhemati/pyising).  The Python host layer (pyising_b200.backend)
+ * binds these through ctypes; INTEGRATION.md shows the binding a pyising maintainer adds.
+ */
+#ifndef ISING_B200_H
+#define ISING_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+#define ISING_OK 0
+#define ISING_ERR_INVALID 1   /* bad argument: shape, variant, algorithm, size, null pointer */
+#define ISING_ERR_CUDA 2      /* a CUDA runtime call failed; message has the CUDA error */
+#define ISING_ERR_NOMEM 3     /* device allocation failed or over the memory budget */
+#define ISING_ERR_TIMEOUT 4   /* a bounded device-side wait expired (kernel returned early) */
+#define ISING_ERR_STATE 5     /* call not valid in the object's current state */
+
+/* ---- enums --------------------------------------------------------------------------- */
+#define ISING_VARIANT_INT8 0  /* compressed checkerboard, one int8 per spin (2D/3D) */
+#define ISING_VARIANT_MSC 1   /* multi-spin coding, 64 spins per uint64 (2D Metropolis) */
+#define ISING_METROPOLIS 0
+#define ISING_HEATBATH 1
+
+typedef struct ising_sim ising_sim;
+
+/* Message of the last failed call on this thread ("" if none).
+ * Replaces: exceptions raised by pyising (src/pyising/lattice.py:25-34,
+ * src/pyising/backends/base.py:54-57, src/pyising/backends/__init__.py:37-38,60-61). */
+const char* ising_last_error(void);
+
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int ising_version(void);
+
+/* Number of visible CUDA devices.
+ * Replaces: pyising.backends._gpu.cuda_available (src/pyising/backends/_gpu.py:39-45). */
+int ising_device_count(int* n);
+
+/* Create a simulation: ndim 2 or 3; shape is (Ly, Lx) or (Lz, Ly, Lx); every extent even and
+ * >= 2; Lx % 8 == 0 (int8) or Lx % 128 == 0 (msc, 2D Metropolis only).  Device arrays are
+ * allocated but not initialised: call ising_set_lattice / ising_upload / ising_fill_cold.
+ * Replaces: IsingSimulation.__init__ + _setup (src/pyising/backends/base.py:44-73;
+ * src/pyising/backends/cupy_backend.py:53-66,114-123) and check_shape
+ * (src/pyising/lattice.py:25-34). */
+int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uint64_t seed,
+                 int device, ising_sim** out);
+
+/* Free the device arrays and the handle (NULL is accepted). */
+int ising_destroy(ising_sim* h);
+
+/* Use an existing CUDA stream (cudaStream_t passed as void*; NULL = the handle's own stream).
+ * The caller keeps the stream alive while the handle uses it. */
+int ising_set_stream(ising_sim* h, void* stream);
+
+/* Acceptance table, uint32[2*ndim+1] indexed by (X + 2 ndim) / 2 (threshold_table,
+ * src/pyising/lattice.py:128-142).  The table is copied.
+ * Replaces: IsingSimulation.set_beta/_upload_table (src/pyising/backends/base.py:79-83,
+ * src/pyising/backends/cupy_backend.py:74-75). */
+int ising_set_table(ising_sim* h, const uint32_t* table, int n);
+
+/* Change the Philox key (seed, 64 bit). */
+int ising_set_seed(ising_sim* h, uint64_t seed);
+
+/* Load / read a full int8 lattice (+1/-1, C order, prod(shape) bytes) from / into host memory.
+ * The colour split (and bit packing for msc) runs on the device.
+ * Replaces: set_lattice / get_lattice (src/pyising/backends/numpy_backend.py:46-51,126-131;
+ * src/pyising/backends/cupy_backend.py:77-82,146-152) with to/from_compressed and
+ * pack/unpack_bits (src/pyising/lattice.py:50-90). */
+int ising_set_lattice(ising_sim* h, const int8_t* full);
+int ising_get_lattice(ising_sim* h, int8_t* full);
+
+/* Copy the two colour arrays in their device layout: int8 (rows, Lx/2) or packed uint64
+ * (rows, Lx/128) — the same arrays as to_compressed / pack_bits produce. */
+int ising_upload(ising_sim* h, const void* c0, const void* c1);
+int ising_download(ising_sim* h, void* c0, void* c1);
+
+/* All spins +1.  Replaces: _fill_cold (src/pyising/backends/base.py:119-120). */
+int ising_fill_cold(ising_sim* h);
+
+/* Run n_sweeps full sweeps (colour 0 then colour 1) with sweep counters t0, t0+1, ...
+ * If measure_every > 0, (M, E) as exact int64 after every measure_every-th sweep are written
+ * to series_out[2*i], series_out[2*i+1] (host memory, n_sweeps / measure_every pairs) and the
+ * call blocks until they are there; otherwise the call only enqueues the work.
+ * Replaces: IsingSimulation.sweep (src/pyising/backends/base.py:85-90) with _half_sweep
+ * (src/pyising/backends/cupy_backend.py:68-72,125-135) and the measurement loop of
+ * pyising.observables.sample (src/pyising/observables.py:61-74). */
+int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
+                int64_t* series_out);
+
+/* One colour's half-sweep with sweep counter t (asynchronous).
+ * Replaces: the _half_sweep hook (src/pyising/backends/base.py:101-103;
+ * src/pyising/backends/cupy_backend.py:68-72,125-135). */
+int ising_half_sweep(ising_sim* h, int color, uint64_t t);
+
+/* Exact magnetisation M = sum s and energy E = -sum_<ij> s_i s_j (blocks until done).
+ * Replaces: observables / magnetization / energy (src/pyising/backends/base.py:125-135;
+ * src/pyising/backends/observables_torch.py:46-111). */
+int ising_observables(ising_sim* h, int64_t* m, int64_t* e);
+
+/* Block until the handle's queued work is done.
+ * Replaces: synchronize (src/pyising/backends/cupy_backend.py:86-87). */
+int ising_sync(ising_sim* h);
+
+/* Bytes of device memory the handle holds (spin arrays and buffers).
+ * Replaces: device_bytes (src/pyising/backends/base.py:137-139). */
+int ising_device_bytes(ising_sim* h, int64_t* bytes);
+
+/* Mean Philox calls per word of the msc kernel over n_sweeps sweeps (also advances the
+ * lattice: t0, t0+1, ...); *mean and *warp_max as in the reference's diagnostic.
+ * Replaces: CupyMultiSpin.philox_calls_per_word (src/pyising/backends/cupy_backend.py:137-144).
+ */
+int ising_msc_calls_per_word(ising_sim* h, uint64_t t0, int64_t n_sweeps, double* mean,
+                             double* warp_max);
+
+/* ---- device probes (roofline ceilings and generator checks) ---------------------------- */
+
+/* Philox4x32-10 throughput of this device in calls/ns (best of `repeats`).
+ * Replaces: bench/roofline.py:59-78 (philox_rate). */
+int ising_philox_rate(int device, int calls_per_thread, int repeats, double* calls_per_ns);
+
+/* out[4*i + k] = word k of Philox4x32-10((q0 + i, c1, c2, c3), (k0, k1)), i < n, computed on
+ * the device (checks the device generator against philox4x32, src/pyising/philox.py:26-51). */
+int ising_philox_range(int device, uint32_t q0, int64_t n, uint32_t c1, uint32_t c2, uint32_t c3,
+                       uint32_t k0, uint32_t k1, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISING_B200_H */

@@ -1,0 +1,186 @@
+"""The B200 backend classes: ``B200Int8`` (int8 checkerboard, 2D/3D, Metropolis and heat bath)
+and ``B200MultiSpin`` (64 spins per uint64, 2D Metropolis).
+
+They implement the pyising simulation interface (src/pyising/backends/base.py:19-139) on top of
+the C ABI of ``libising_b200.so``; every sweep, measurement and layout conversion runs in the
+sm_100a kernels, and ``sweep(n)`` issues all ``2n`` half-sweeps in one C call.  Results are
+bit-identical to pyising's NumPy backend (src/pyising/backends/numpy_backend.py) for the same
+seed and start.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import ClassVar
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .base import IsingSimulation
+
+
+def default_device() -> int:
+    return int(os.environ.get("PYISING_B200_DEVICE", "0"))
+
+
+class _B200Simulation(IsingSimulation):
+    backend: ClassVar[str] = "b200"
+    gpu: ClassVar[bool] = True
+    _variant_code: ClassVar[int] = 0
+
+    def _setup(self) -> None:
+        self._h = ctypes.c_void_p()
+        shape = (ctypes.c_int64 * 3)(*(list(self.shape) + [0] * (3 - self.ndim)))
+        self.device = default_device()
+        check(lib().ising_create(self.ndim, shape, self._variant_code,
+                                 _lib.ALGORITHM[self.algorithm], self.seed, self.device,
+                                 ctypes.byref(self._h)), "create")
+        self._upload_table()
+
+    def __del__(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().ising_destroy(h)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
+            self._h = None
+
+    # ---- hooks -------------------------------------------------------------------------------
+    def _upload_table(self) -> None:
+        tab = np.ascontiguousarray(self.table, dtype=np.uint32)
+        check(lib().ising_set_table(self._h, tab.ctypes.data, len(tab)), "set_table")
+
+    def _half_sweep(self, color: int) -> None:
+        check(lib().ising_half_sweep(self._h, int(color), self.t), "half_sweep")
+
+    def _fill_cold(self) -> None:
+        check(lib().ising_fill_cold(self._h), "fill_cold")
+
+    def set_lattice(self, lat: np.ndarray) -> None:
+        full = np.ascontiguousarray(np.asarray(lat, dtype=np.int8).reshape(self.shape))
+        check(lib().ising_set_lattice(self._h, full.ctypes.data), "set_lattice")
+
+    def get_lattice(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.int8)
+        check(lib().ising_get_lattice(self._h, out.ctypes.data), "get_lattice")
+        return out
+
+    def synchronize(self) -> None:
+        check(lib().ising_sync(self._h), "sync")
+
+    # ---- the hot path -----------------------------------------------------------------------
+    def sweep(self, n: int = 1) -> None:
+        """``n`` full sweeps in one C call (asynchronous; ``self.t`` advances by ``n``)."""
+        n = int(n)
+        if n <= 0:
+            return
+        check(lib().ising_sweep(self._h, self.t, n, 0, None), "sweep")
+        self.t += n
+
+    def sweep_measured(self, n: int, every: int) -> np.ndarray:
+        """``n`` sweeps with exact ``(M, E)`` after every ``every``-th one, measured inside the
+        colour-1 half-sweep; returns an int64 array of shape ``(n // every, 2)``.  This is the
+        device-resident form of pyising.observables.sample (src/pyising/observables.py:61-74)."""
+        n, every = int(n), int(every)
+        if every <= 0:
+            raise ValueError("every must be positive")
+        out = np.zeros((n // every, 2), dtype=np.int64)
+        check(lib().ising_sweep(self._h, self.t, n, every, out.ctypes.data), "sweep")
+        self.t += n
+        return out
+
+    def observables_int(self) -> tuple[int, int]:
+        """Exact integers ``(M, E)``: ``M = sum s``, ``E = -sum_<ij> s_i s_j``."""
+        m, e = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().ising_observables(self._h, ctypes.byref(m), ctypes.byref(e)), "observables")
+        return int(m.value), int(e.value)
+
+    def observables(self) -> tuple[float, float]:
+        """``(m, e)`` per spin, as pyising's GPU backends return them."""
+        m, e = self.observables_int()
+        return m / self.n_spins, e / self.n_spins
+
+    def magnetization(self) -> float:
+        return self.observables()[0]
+
+    def energy(self) -> float:
+        return self.observables()[1]
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_int64()
+        check(lib().ising_device_bytes(self._h, ctypes.byref(b)), "device_bytes")
+        return int(b.value)
+
+    def set_seed(self, seed: int) -> None:
+        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        check(lib().ising_set_seed(self._h, self.seed), "set_seed")
+
+    def set_stream(self, stream: int | None) -> None:
+        """Issue work on an existing CUDA stream (e.g. ``torch.cuda.current_stream().cuda_stream``)."""
+        check(lib().ising_set_stream(self._h, stream or None), "set_stream")
+
+    # ---- checkpoint / resume -----------------------------------------------------------------
+    def colour_arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        """The two colour arrays in their device layout (compressed int8 or packed uint64)."""
+        a, b = self._colour_buffers()
+        check(lib().ising_download(self._h, a.ctypes.data, b.ctypes.data), "download")
+        return a, b
+
+    def load_colour_arrays(self, c0: np.ndarray, c1: np.ndarray) -> None:
+        a, b = self._colour_buffers()
+        a[...] = c0
+        b[...] = c1
+        check(lib().ising_upload(self._h, a.ctypes.data, b.ctypes.data), "upload")
+
+    def state(self) -> dict:
+        """Everything needed to resume bit-exactly: the RNG is keyed by (site, t, colour, seed)."""
+        c0, c1 = self.colour_arrays()
+        return {"shape": self.shape, "variant": self.variant, "algorithm": self.algorithm,
+                "beta": self.beta, "seed": self.seed, "t": self.t, "c0": c0, "c1": c1}
+
+    @classmethod
+    def from_state(cls, st: dict) -> _B200Simulation:
+        sim = cls(st["shape"], st["beta"], seed=st["seed"], algorithm=st["algorithm"],
+                  init="cold")
+        sim.load_colour_arrays(st["c0"], st["c1"])
+        sim.t = int(st["t"])
+        return sim
+
+
+class B200Int8(_B200Simulation):
+    """int8 compressed checkerboard (2D/3D, Metropolis and heat bath)."""
+
+    variant = "int8"
+    stream = "int8"
+    _variant_code = 0
+
+    def _colour_buffers(self):
+        return (np.empty((self.rows, self.lh), np.int8), np.empty((self.rows, self.lh), np.int8))
+
+
+class B200MultiSpin(_B200Simulation):
+    """Multi-spin coding: 64 spins per uint64, bit-sliced neighbour count, lazy comparison."""
+
+    variant = "msc"
+    dims = (2,)
+    algorithms = ("metropolis",)
+    layout_multiple = 128
+    stream = "msc"
+    bytes_per_update = 3.0 / 8.0
+    _variant_code = 1
+
+    def _colour_buffers(self):
+        nw = self.lh // 64
+        return (np.empty((self.rows, nw), np.uint64), np.empty((self.rows, nw), np.uint64))
+
+    def philox_calls_per_word(self, sweeps: int = 2, warp: bool = False) -> float:
+        """Mean (or per-warp maximum) Philox calls per word; advances the lattice like
+        ``sweep(sweeps)`` (src/pyising/backends/cupy_backend.py:137-144)."""
+        mean, wmax = ctypes.c_double(), ctypes.c_double()
+        check(lib().ising_msc_calls_per_word(self._h, self.t, int(sweeps), ctypes.byref(mean),
+                                             ctypes.byref(wmax)), "calls_per_word")
+        self.t += int(sweeps)
+        return float(wmax.value if warp else mean.value)

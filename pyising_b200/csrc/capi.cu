@@ -1,0 +1,563 @@
+// C ABI (include/ising_b200.h): handle management, layout transfers, the sweep loop and the
+// device probes.  All device work of a handle runs on its stream.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "capi_internal.h"
+
+namespace ising {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(ISING_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+int device_sm_count(int device)
+{
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return 148;
+    return n > 0 ? n : 148;
+}
+
+int select_rule(int variant, int algorithm, int ndim, const u32* table)
+{
+    if (variant == ISING_VARIANT_MSC) return kMetroFast;
+    const int d = ndim;
+    if (algorithm == ISING_METROPOLIS) {
+        // the fast rule needs T(a) = table[2d - a] non-decreasing in a < d
+        for (int i = d + 1; i < 2 * d; ++i)
+            if (table[i] < table[i + 1]) return kMetroGeneric;
+        return kMetroFast;
+    }
+    for (int i = 0; i < 2 * d; ++i)
+        if (table[i] > table[i + 1]) return kHeatGeneric;
+    return kHeatFast;
+}
+
+}  // namespace ising
+
+using namespace ising;
+
+#define TRY_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+#define CHECK_HANDLE(h)                                                    \
+    do {                                                                   \
+        if (!(h)) return fail(ISING_ERR_INVALID, "null simulation handle"); \
+    } while (0)
+
+extern "C" {
+
+const char* ising_last_error(void) { return g_last_error.c_str(); }
+
+int ising_version(void) { return 100; }
+
+int ising_device_count(int* n)
+{
+    if (!n) return fail(ISING_ERR_INVALID, "null output pointer");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        *n = 0;
+        cudaGetLastError();
+        return cuda_fail(e, "cudaGetDeviceCount");
+    }
+    *n = c;
+    return ISING_OK;
+}
+
+int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uint64_t seed,
+                 int device, ising_sim** out)
+{
+    if (!out || !shape) return fail(ISING_ERR_INVALID, "null pointer argument");
+    *out = nullptr;
+    if (ndim != 2 && ndim != 3)
+        return fail(ISING_ERR_INVALID, "only 2D and 3D lattices are supported, got ndim=%d", ndim);
+    for (int i = 0; i < ndim; ++i)
+        if (shape[i] < 2 || shape[i] % 2)
+            return fail(ISING_ERR_INVALID, "all extents must be even and >= 2");
+    if (variant != ISING_VARIANT_INT8 && variant != ISING_VARIANT_MSC)
+        return fail(ISING_ERR_INVALID, "unknown variant %d", variant);
+    if (algorithm != ISING_METROPOLIS && algorithm != ISING_HEATBATH)
+        return fail(ISING_ERR_INVALID, "unknown algorithm %d", algorithm);
+    const int64_t lx = shape[ndim - 1];
+    const int multiple = variant == ISING_VARIANT_MSC ? 128 : 8;
+    if (lx % multiple)
+        return fail(ISING_ERR_INVALID, "last extent must be a multiple of %d, got %lld", multiple,
+                    (long long)lx);
+    if (variant == ISING_VARIANT_MSC && (ndim != 2 || algorithm != ISING_METROPOLIS))
+        return fail(ISING_ERR_INVALID, "msc supports 2D Metropolis only");
+    const int64_t ly = shape[ndim - 2];
+    const int64_t lz = ndim == 3 ? shape[0] : 1;
+    const int64_t rows = ly * lz;
+    if (rows > (int64_t)0x7FFFFFFF || lx / 2 > (int64_t)0x7FFFFFFF)
+        return fail(ISING_ERR_INVALID, "lattice too large for 32-bit row indices");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(ISING_ERR_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev)
+        return fail(ISING_ERR_INVALID, "device %d out of range (%d devices)", device, ndev);
+    TRY_CUDA(cudaSetDevice(device));
+
+    ising_sim* h = new ising_sim();
+    h->device = device;
+    h->ndim = ndim;
+    h->variant = variant;
+    h->algorithm = algorithm;
+    for (int i = 0; i < 3; ++i) h->shape[i] = i < ndim ? shape[i] : 0;
+    h->rows = rows;
+    h->lh = (int)(lx / 2);
+    h->ly = (int)ly;
+    h->lz = (int)lz;
+    h->nw = (int)(lx / 128);
+    h->seed = seed;
+    h->table_n = 2 * ndim + 1;
+    for (int i = 0; i < 7; ++i) h->table[i] = 0xFFFFFFFFu;
+    h->rule = select_rule(variant, algorithm, ndim, h->table);
+    h->sm_count = device_sm_count(device);
+    h->max_blocks = h->sm_count * 8;
+    h->colour_bytes = variant == ISING_VARIANT_MSC ? (size_t)rows * h->nw * 8
+                                                  : (size_t)rows * (size_t)h->lh;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->own_stream_handle, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    h->stream = h->own_stream_handle;
+    for (int c = 0; c < 2; ++c) {
+        e = cudaMalloc(&h->c[c], h->colour_bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ising_destroy(h);
+            return fail(ISING_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", h->colour_bytes,
+                        cudaGetErrorString(e));
+        }
+    }
+    e = cudaMalloc(&h->d_acc, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ising_destroy(h);
+        return fail(ISING_ERR_NOMEM, "cudaMalloc of the accumulators failed");
+    }
+    *out = h;
+    return ISING_OK;
+}
+
+int ising_destroy(ising_sim* h)
+{
+    if (!h) return ISING_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int c = 0; c < 2; ++c)
+        if (h->c[c]) cudaFree(h->c[c]);
+    if (h->d_acc) cudaFree(h->d_acc);
+    if (h->d_series) cudaFree(h->d_series);
+    if (h->h_series) cudaFreeHost(h->h_series);
+    if (h->own_stream_handle) cudaStreamDestroy(h->own_stream_handle);
+    cudaGetLastError();
+    delete h;
+    return ISING_OK;
+}
+
+int ising_set_stream(ising_sim* h, void* stream)
+{
+    CHECK_HANDLE(h);
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream_handle;
+    return ISING_OK;
+}
+
+int ising_set_table(ising_sim* h, const uint32_t* table, int n)
+{
+    CHECK_HANDLE(h);
+    if (!table) return fail(ISING_ERR_INVALID, "null table");
+    if (n != h->table_n)
+        return fail(ISING_ERR_INVALID, "table must have %d entries, got %d", h->table_n, n);
+    for (int i = 0; i < 7; ++i) h->table[i] = i < n ? table[i] : 0xFFFFFFFFu;
+    h->rule = select_rule(h->variant, h->algorithm, h->ndim, h->table);
+    return ISING_OK;
+}
+
+int ising_set_seed(ising_sim* h, uint64_t seed)
+{
+    CHECK_HANDLE(h);
+    h->seed = seed;
+    return ISING_OK;
+}
+
+// Full lattices move through a bounded device staging buffer, a block of rows at a time.
+static const size_t kStagingBytes = (size_t)256 << 20;
+
+static long long rows_per_chunk(const ising_sim* h)
+{
+    const size_t row_bytes = (size_t)2 * h->lh;
+    long long r = (long long)(kStagingBytes / row_bytes);
+    if (r < 1) r = 1;
+    if (h->variant == ISING_VARIANT_MSC && r > 1) r &= ~1LL;  // keep row parity aligned
+    return r > h->rows ? h->rows : r;
+}
+
+int ising_set_lattice(ising_sim* h, const int8_t* full)
+{
+    CHECK_HANDLE(h);
+    if (!full) return fail(ISING_ERR_INVALID, "null lattice");
+    TRY_CUDA(cudaSetDevice(h->device));
+    const long long rpc = rows_per_chunk(h);
+    const size_t row_bytes = (size_t)2 * h->lh;
+    int8_t* stage = nullptr;
+    TRY_CUDA(cudaMallocAsync((void**)&stage, rpc * row_bytes, h->stream));
+    int rc = ISING_OK;
+    for (long long r0 = 0; r0 < h->rows && rc == ISING_OK; r0 += rpc) {
+        const long long nr = (r0 + rpc > h->rows) ? h->rows - r0 : rpc;
+        cudaError_t e = cudaMemcpyAsync(stage, full + r0 * row_bytes, nr * row_bytes,
+                                        cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) {
+            if (h->variant == ISING_VARIANT_MSC)
+                e = launch_msc_pack(stage, (u64*)h->c[0] + r0 * h->nw,
+                                    (u64*)h->c[1] + r0 * h->nw, (int)nr, (int)r0, h->nw,
+                                    h->max_blocks, h->stream);
+            else
+                e = launch_int8_split(stage, (int8_t*)h->c[0] + r0 * h->lh,
+                                      (int8_t*)h->c[1] + r0 * h->lh, nr, r0, h->lh, h->ly,
+                                      h->max_blocks, h->stream);
+        }
+        if (e != cudaSuccess) rc = cuda_fail(e, "set_lattice");
+    }
+    cudaFreeAsync(stage, h->stream);
+    if (rc == ISING_OK) TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return rc;
+}
+
+int ising_get_lattice(ising_sim* h, int8_t* full)
+{
+    CHECK_HANDLE(h);
+    if (!full) return fail(ISING_ERR_INVALID, "null lattice");
+    TRY_CUDA(cudaSetDevice(h->device));
+    const long long rpc = rows_per_chunk(h);
+    const size_t row_bytes = (size_t)2 * h->lh;
+    int8_t* stage = nullptr;
+    TRY_CUDA(cudaMallocAsync((void**)&stage, rpc * row_bytes, h->stream));
+    int rc = ISING_OK;
+    for (long long r0 = 0; r0 < h->rows && rc == ISING_OK; r0 += rpc) {
+        const long long nr = (r0 + rpc > h->rows) ? h->rows - r0 : rpc;
+        cudaError_t e;
+        if (h->variant == ISING_VARIANT_MSC)
+            e = launch_msc_unpack((const u64*)h->c[0] + r0 * h->nw,
+                                  (const u64*)h->c[1] + r0 * h->nw, stage, (int)nr, (int)r0,
+                                  h->nw, h->max_blocks, h->stream);
+        else
+            e = launch_int8_merge((const int8_t*)h->c[0] + r0 * h->lh,
+                                  (const int8_t*)h->c[1] + r0 * h->lh, stage, nr, r0, h->lh,
+                                  h->ly, h->max_blocks, h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(full + r0 * row_bytes, stage, nr * row_bytes,
+                                cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "get_lattice");
+    }
+    cudaFreeAsync(stage, h->stream);
+    cudaStreamSynchronize(h->stream);
+    return rc;
+}
+
+int ising_upload(ising_sim* h, const void* c0, const void* c1)
+{
+    CHECK_HANDLE(h);
+    if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
+    TRY_CUDA(cudaSetDevice(h->device));
+    TRY_CUDA(cudaMemcpyAsync(h->c[0], c0, h->colour_bytes, cudaMemcpyHostToDevice, h->stream));
+    TRY_CUDA(cudaMemcpyAsync(h->c[1], c1, h->colour_bytes, cudaMemcpyHostToDevice, h->stream));
+    TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return ISING_OK;
+}
+
+int ising_download(ising_sim* h, void* c0, void* c1)
+{
+    CHECK_HANDLE(h);
+    if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
+    TRY_CUDA(cudaSetDevice(h->device));
+    TRY_CUDA(cudaMemcpyAsync(c0, h->c[0], h->colour_bytes, cudaMemcpyDeviceToHost, h->stream));
+    TRY_CUDA(cudaMemcpyAsync(c1, h->c[1], h->colour_bytes, cudaMemcpyDeviceToHost, h->stream));
+    TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return ISING_OK;
+}
+
+int ising_fill_cold(ising_sim* h)
+{
+    CHECK_HANDLE(h);
+    TRY_CUDA(cudaSetDevice(h->device));
+    const int v = h->variant == ISING_VARIANT_MSC ? 0xFF : 0x01;
+    for (int c = 0; c < 2; ++c) TRY_CUDA(cudaMemsetAsync(h->c[c], v, h->colour_bytes, h->stream));
+    return ISING_OK;
+}
+
+int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
+                int64_t* series_out)
+{
+    CHECK_HANDLE(h);
+    if (n_sweeps < 0) return fail(ISING_ERR_INVALID, "negative sweep count");
+    if (measure_every < 0) return fail(ISING_ERR_INVALID, "negative measurement interval");
+    if (measure_every > 0 && !series_out)
+        return fail(ISING_ERR_INVALID, "measure_every > 0 needs series_out");
+    TRY_CUDA(cudaSetDevice(h->device));
+    const int64_t n_meas = measure_every > 0 ? n_sweeps / measure_every : 0;
+    if (n_meas > 0) {
+        int rc = ensure_series(h, n_meas);
+        if (rc != ISING_OK) return rc;
+        TRY_CUDA(cudaMemsetAsync(h->d_series, 0, (size_t)n_meas * 2 * sizeof(long long),
+                                 h->stream));
+    }
+    int64_t k = 0;
+    for (int64_t s = 0; s < n_sweeps; ++s) {
+        const u32 t = (u32)(t0 + (uint64_t)s);
+        const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;
+        unsigned long long* m = meas ? (unsigned long long*)(h->d_series + 2 * k) : nullptr;
+        int rc = half_sweep(h, 0, t, nullptr, nullptr);
+        if (rc == ISING_OK) rc = half_sweep(h, 1, t, m, nullptr);
+        if (rc != ISING_OK) return rc;
+        if (meas) ++k;
+    }
+    if (n_meas > 0) {
+        TRY_CUDA(cudaMemcpyAsync(h->h_series, h->d_series, (size_t)n_meas * 2 * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        TRY_CUDA(cudaStreamSynchronize(h->stream));
+        memcpy(series_out, h->h_series, (size_t)n_meas * 2 * sizeof(long long));
+    }
+    return ISING_OK;
+}
+
+int ising_half_sweep(ising_sim* h, int color, uint64_t t)
+{
+    CHECK_HANDLE(h);
+    if (color != 0 && color != 1) return fail(ISING_ERR_INVALID, "colour must be 0 or 1");
+    TRY_CUDA(cudaSetDevice(h->device));
+    return half_sweep(h, color, (u32)t, nullptr, nullptr);
+}
+
+int ising_observables(ising_sim* h, int64_t* m, int64_t* e)
+{
+    CHECK_HANDLE(h);
+    if (!m || !e) return fail(ISING_ERR_INVALID, "null output pointer");
+    TRY_CUDA(cudaSetDevice(h->device));
+    TRY_CUDA(cudaMemsetAsync(h->d_acc, 0, 2 * sizeof(unsigned long long), h->stream));
+    int rc = observe(h, h->d_acc);
+    if (rc != ISING_OK) return rc;
+    long long out[2];
+    TRY_CUDA(cudaMemcpyAsync(out, h->d_acc, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    TRY_CUDA(cudaStreamSynchronize(h->stream));
+    *m = out[0];
+    *e = out[1];
+    return ISING_OK;
+}
+
+int ising_sync(ising_sim* h)
+{
+    CHECK_HANDLE(h);
+    TRY_CUDA(cudaSetDevice(h->device));
+    TRY_CUDA(cudaStreamSynchronize(h->stream));
+    return ISING_OK;
+}
+
+int ising_device_bytes(ising_sim* h, int64_t* bytes)
+{
+    CHECK_HANDLE(h);
+    if (!bytes) return fail(ISING_ERR_INVALID, "null output pointer");
+    *bytes = (int64_t)(2 * h->colour_bytes + 8 * sizeof(unsigned long long) +
+                       (size_t)h->series_cap * 2 * sizeof(long long));
+    return ISING_OK;
+}
+
+int ising_msc_calls_per_word(ising_sim* h, uint64_t t0, int64_t n_sweeps, double* mean,
+                             double* warp_max)
+{
+    CHECK_HANDLE(h);
+    if (h->variant != ISING_VARIANT_MSC) return fail(ISING_ERR_INVALID, "not an msc simulation");
+    if (n_sweeps <= 0 || !mean || !warp_max) return fail(ISING_ERR_INVALID, "bad arguments");
+    TRY_CUDA(cudaSetDevice(h->device));
+    unsigned long long* stats = h->d_acc + 2;
+    TRY_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), h->stream));
+    for (int64_t s = 0; s < n_sweeps; ++s) {
+        const u32 t = (u32)(t0 + (uint64_t)s);
+        int rc = half_sweep(h, 0, t, nullptr, stats);
+        if (rc == ISING_OK) rc = half_sweep(h, 1, t, nullptr, stats);
+        if (rc != ISING_OK) return rc;
+    }
+    unsigned long long out[2];
+    TRY_CUDA(cudaMemcpyAsync(out, stats, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    TRY_CUDA(cudaStreamSynchronize(h->stream));
+    const double words = 2.0 * (double)n_sweeps * (double)h->rows * (double)h->nw;
+    *mean = (double)out[0] / words;
+    *warp_max = (double)out[1] / words;
+    return ISING_OK;
+}
+
+int ising_philox_rate(int device, int calls_per_thread, int repeats, double* calls_per_ns)
+{
+    if (!calls_per_ns || calls_per_thread <= 0 || repeats <= 0)
+        return fail(ISING_ERR_INVALID, "bad arguments");
+    TRY_CUDA(cudaSetDevice(device));
+    const int sms = device_sm_count(device);
+    const int threads = 256, blocks = sms * 8 * 4;
+    u32* out = nullptr;
+    TRY_CUDA(cudaMalloc(&out, (size_t)threads * blocks * sizeof(u32)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    double best = 0.0;
+    cudaError_t e = launch_philox_probe(out, blocks, threads, calls_per_thread, 1u, 2u, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    for (int i = 0; i < repeats && e == cudaSuccess; ++i) {
+        cudaEventRecord(a, 0);
+        e = launch_philox_probe(out, blocks, threads, calls_per_thread, 1u, 2u, 0);
+        cudaEventRecord(b, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double rate = (double)threads * blocks * calls_per_thread / (ms * 1e6);
+        if (rate > best) best = rate;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess) return cuda_fail(e, "philox probe");
+    *calls_per_ns = best;
+    return ISING_OK;
+}
+
+int ising_philox_range(int device, uint32_t q0, int64_t n, uint32_t c1, uint32_t c2, uint32_t c3,
+                       uint32_t k0, uint32_t k1, uint32_t* out)
+{
+    if (!out || n < 0) return fail(ISING_ERR_INVALID, "bad arguments");
+    if (n == 0) return ISING_OK;
+    TRY_CUDA(cudaSetDevice(device));
+    u32* d = nullptr;
+    TRY_CUDA(cudaMalloc(&d, (size_t)n * 16));
+    cudaError_t e = launch_philox_range(d, n, q0, c1, c2, c3, k0, k1,
+                                        device_sm_count(device) * 8, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, (size_t)n * 16, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "philox range");
+    return ISING_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- internal helpers --------
+namespace ising {
+
+int ensure_series(ising_sim* h, int64_t pairs)
+{
+    if (pairs <= h->series_cap) return ISING_OK;
+    if (h->d_series) cudaFree(h->d_series);
+    if (h->h_series) cudaFreeHost(h->h_series);
+    h->d_series = nullptr;
+    h->h_series = nullptr;
+    h->series_cap = 0;
+    const size_t bytes = (size_t)pairs * 2 * sizeof(long long);
+    cudaError_t e = cudaMalloc(&h->d_series, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ISING_ERR_NOMEM, "cudaMalloc of %zu series bytes failed", bytes);
+    }
+    e = cudaMallocHost(&h->h_series, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ISING_ERR_NOMEM, "cudaMallocHost of %zu bytes failed", bytes);
+    }
+    h->series_cap = pairs;
+    return ISING_OK;
+}
+
+int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
+               unsigned long long* stats)
+{
+    const u32 k0 = (u32)h->seed, k1 = (u32)(h->seed >> 32);
+    cudaError_t e;
+    if (h->variant == ISING_VARIANT_MSC) {
+        MscHalf p;
+        p.own = (u64*)h->c[color];
+        p.other = (const u64*)h->c[1 - color];
+        p.rows = (int)h->rows;
+        p.nw = h->nw;
+        p.t = t;
+        p.color = (u32)color;
+        p.k0 = k0;
+        p.k1 = k1;
+        p.thr4 = h->table[3];
+        p.thr8 = h->table[4];
+        p.meas = meas;
+        p.stats = stats;
+        e = launch_msc_half(true, p, h->max_blocks, h->stream);
+    } else {
+        Int8Half p;
+        p.own = (int8_t*)h->c[color];
+        p.other = (const int8_t*)h->c[1 - color];
+        p.rows = h->rows;
+        p.lh = h->lh;
+        p.ly = h->ly;
+        p.lz = h->lz;
+        p.cpr = h->lh / int8_chunk_width(h->lh);
+        p.t = t;
+        p.color = (u32)color;
+        p.k0 = k0;
+        p.k1 = k1;
+        for (int i = 0; i < 7; ++i) p.table[i] = h->table[i];
+        p.meas = meas;
+        e = launch_int8_half(h->ndim, h->rule, p, h->max_blocks, h->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "half-sweep launch");
+    return ISING_OK;
+}
+
+int observe(ising_sim* h, unsigned long long* acc)
+{
+    cudaError_t e;
+    if (h->variant == ISING_VARIANT_MSC) {
+        MscHalf p;
+        memset(&p, 0, sizeof p);
+        p.own = (u64*)h->c[1];
+        p.other = (const u64*)h->c[0];
+        p.rows = (int)h->rows;
+        p.nw = h->nw;
+        p.color = 1;
+        p.meas = acc;
+        e = launch_msc_half(false, p, h->max_blocks, h->stream);
+    } else {
+        Int8Half p;
+        memset(&p, 0, sizeof p);
+        p.own = (int8_t*)h->c[1];
+        p.other = (const int8_t*)h->c[0];
+        p.rows = h->rows;
+        p.lh = h->lh;
+        p.ly = h->ly;
+        p.lz = h->lz;
+        p.cpr = h->lh / int8_chunk_width(h->lh);
+        p.color = 1;
+        p.meas = acc;
+        e = launch_int8_half(h->ndim, kObserve, p, h->max_blocks, h->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "observables launch");
+    return ISING_OK;
+}
+
+}  // namespace ising

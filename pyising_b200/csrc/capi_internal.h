@@ -1,0 +1,69 @@
+// Internal declarations shared by the C-ABI translation units (not part of the public ABI).
+#pragma once
+
+#include <string>
+
+#include "common.cuh"
+#include "ising_b200.h"
+
+// A simulation handle: one lattice, its two colour arrays on one device, one stream.
+struct ising_sim {
+    int device = 0;
+    int ndim = 2;
+    int variant = ISING_VARIANT_INT8;
+    int algorithm = ISING_METROPOLIS;
+    int64_t shape[3] = {0, 0, 0};
+    long long rows = 0;  // prod(shape[:-1])
+    int lh = 0;          // Lx / 2
+    int ly = 0;          // rows per plane
+    int lz = 1;          // planes (1 in 2D)
+    int nw = 0;          // packed words per row (msc)
+    uint64_t seed = 0;
+    uint32_t table[7] = {0, 0, 0, 0, 0, 0, 0};
+    int table_n = 5;
+    int rule = 0;        // ising::Rule chosen from the table
+    void* c[2] = {nullptr, nullptr};
+    size_t colour_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream_handle = nullptr;
+    unsigned long long* d_acc = nullptr;  // [0,1] observables, [2,3] msc call statistics
+    long long* d_series = nullptr;        // (M, E) pairs of one ising_sweep call
+    long long* h_series = nullptr;        // pinned copy of d_series
+    int64_t series_cap = 0;               // pairs
+    int sm_count = 148;
+    int max_blocks = 148 * 8;
+};
+
+namespace ising {
+
+extern thread_local std::string g_last_error;
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+int device_sm_count(int device);
+int select_rule(int variant, int algorithm, int ndim, const u32* table);
+
+int ensure_series(ising_sim* h, int64_t pairs);
+int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
+               unsigned long long* stats);
+int observe(ising_sim* h, unsigned long long* acc);
+
+// kernel launchers
+int int8_chunk_width(int lh);
+void int8_geometry(long long rows, int cpr, int max_blocks, dim3* grid, dim3* block);
+cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_blocks,
+                             cudaStream_t st);
+cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st);
+cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,
+                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st);
+cudaError_t launch_int8_merge(const int8_t* c0, const int8_t* c1, int8_t* full, long long rows,
+                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st);
+cudaError_t launch_msc_pack(const int8_t* full, u64* w0, u64* w1, int rows, int row0, int nw,
+                            int max_blocks, cudaStream_t st);
+cudaError_t launch_msc_unpack(const u64* w0, const u64* w1, int8_t* full, int rows, int row0,
+                              int nw, int max_blocks, cudaStream_t st);
+cudaError_t launch_philox_probe(u32* out, int blocks, int threads, int calls, u32 k0, u32 k1,
+                                cudaStream_t st);
+cudaError_t launch_philox_range(u32* out, long long n, u32 q0, u32 c1, u32 c2, u32 c3, u32 k0,
+                                u32 k1, int max_blocks, cudaStream_t st);
+
+}  // namespace ising

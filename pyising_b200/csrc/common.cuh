@@ -1,0 +1,133 @@
+// Shared device code: Philox4x32-10, SWAR helpers, reductions and launch-parameter structs.
+//
+// Philox4x32-10 follows Salmon et al., SC'11 (the published Random123 algorithm) with the
+// counter/key conventions of pyising's oracle: src/pyising/philox.py:26-51 (multipliers,
+// Weyl key increments, key bumped between rounds but not after the last one).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ising {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+
+constexpr u32 kPhiloxM0 = 0xD2511F53u;
+constexpr u32 kPhiloxM1 = 0xCD9E8D57u;
+constexpr u32 kPhiloxW0 = 0x9E3779B9u;
+constexpr u32 kPhiloxW1 = 0xBB67AE85u;
+
+struct u32x4 {
+    u32 x, y, z, w;
+};
+
+// One Philox4x32-10 block.  The counter words c1..c3 and the key are usually uniform across a
+// warp (sweep, colour, stream selector, seed), so the compiler keeps the first two rounds'
+// products in the uniform datapath; only the site/word index c0 varies per thread.
+__device__ __forceinline__ u32x4 philox4x32_10(u32 c0, u32 c1, u32 c2, u32 c3, u32 k0, u32 k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const u64 p0 = (u64)kPhiloxM0 * c0;
+        const u64 p1 = (u64)kPhiloxM1 * c2;
+        const u32 n0 = (u32)(p1 >> 32) ^ c1 ^ k0;
+        const u32 n2 = (u32)(p0 >> 32) ^ c3 ^ k1;
+        c1 = (u32)p1;
+        c3 = (u32)p0;
+        c0 = n0;
+        c2 = n2;
+        k0 += kPhiloxW0;
+        k1 += kPhiloxW1;
+    }
+    return u32x4{c0, c1, c2, c3};
+}
+
+// Byte lanes of packed int8 spins: +1 is 0x01, -1 is 0xFF, so bit 1 of a byte is the
+// "spin down" flag and (a ^ b) & 0x02 is the "anti-aligned" flag of two spins.
+constexpr u32 kBit1 = 0x02020202u;
+constexpr u32 kBit7 = 0x80808080u;
+
+// 0x80 per selected byte -> 0xFE per selected byte (the XOR that flips a +-1 byte).
+__device__ __forceinline__ u32 flip_mask_from_bit7(u32 m7) { return m7 | (m7 - (m7 >> 6)); }
+
+// Sum of the four bytes of v (each byte small and non-negative).
+__device__ __forceinline__ int byte_sum(u32 v) { return (int)__dp4a(v, 0x01010101u, 0u); }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// Block-wide sum of two int64 values, then one atomicAdd per block into out[0], out[1].
+// Every thread of the block must call it.
+__device__ __forceinline__ void block_accumulate2(long long a, long long b,
+                                                  unsigned long long* out)
+{
+    __shared__ long long sa[32], sb[32];
+    const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+    const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+    const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+    __syncthreads();  // a previous call's readers of sa/sb are done
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        sa[warp] = a;
+        sb[warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        a = lane < nwarps ? sa[lane] : 0;
+        b = lane < nwarps ? sb[lane] : 0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (lane == 0) {
+            atomicAdd(out, (unsigned long long)a);
+            atomicAdd(out + 1, (unsigned long long)b);
+        }
+    }
+}
+
+// Decision rule selected on the host.
+enum Rule : int {
+    kMetroFast = 0,    // Metropolis, table[d+1..2d] non-increasing (always true for tables
+                       // built by threshold_table)
+    kHeatFast = 1,     // heat bath, table non-decreasing (beta >= 0)
+    kMetroGeneric = 2, // any table, one lookup per site
+    kHeatGeneric = 3,
+    kObserve = 4,      // no update: measurement only
+};
+
+// Parameters of one int8 half-sweep launch over a (rows, lh) colour array pair.
+struct Int8Half {
+    int8_t* own;
+    const int8_t* other;
+    long long rows;
+    int lh;      // Lx / 2 (bytes per row)
+    int ly;      // rows per z plane
+    int lz;      // planes (1 in 2D)
+    int cpr;     // chunks per row = lh / V
+    u32 t;       // sweep counter (Philox counter word 1)
+    u32 color;   // colour being updated (Philox counter word 2)
+    u32 k0, k1;  // Philox key (seed lo, hi)
+    u32 table[7];
+    unsigned long long* meas;  // (M, E) accumulators, or nullptr
+};
+
+// Parameters of one packed (msc) half-sweep launch over (rows, nw) uint64 words.
+struct MscHalf {
+    u64* own;
+    const u64* other;
+    int rows;
+    int nw;     // words per row = Lx / 128
+    u32 t, color, k0, k1;
+    u32 thr4;   // table[3]: acceptance for one anti-aligned neighbour (dE = 4)
+    u32 thr8;   // table[4]: acceptance for none (dE = 8)
+    unsigned long long* meas;   // (M, E) accumulators, or nullptr
+    unsigned long long* stats;  // (calls, warp-max calls) diagnostics, or nullptr
+};
+
+}  // namespace ising
