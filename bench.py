@@ -1,0 +1,446 @@
+"""Benchmark of the pyising sweep hot path on B200: one JSON line on stdout (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload msc16384|int8_1024|int8_3d_256] [--no-extras]
+
+Headline workload (one "step" = one whole job of the config): 2D multi-spin-coded Metropolis,
+L = 16384 (64 spins per uint64, 16384 x 128 words per colour), periodic, T = T_c, hot start
+seed 7 (pyising's NumPy hot start), 1000 sweeps.  ``value`` is flips/ns (attempted spin updates
+per ns) with the lattice resident in HBM; ``e2e`` is the same job through the public Python API
+with the lattice uploaded from and downloaded to host memory inside the timed region.
+The L2 cache (126 MB) is flushed between steps by writing a 256 MiB buffer; within a step the
+32 MiB lattice stays L2-resident, which is part of the workload.
+
+Under torchrun (N > 1) every rank runs its own replica (seed 7 + rank; no collective on the data
+path): ``value`` is the flips of all ranks / the slowest rank's time ("scaling": "weak").
+
+``--impl reference`` times the CPU restatement of the reference's algorithm (oracle/, the NumPy
+backend's algorithm in C, all host threads) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BETA_C_2D = math.log(1.0 + math.sqrt(2.0)) / 2.0
+BETA_3D = 0.221654626
+L2_FLUSH_BYTES = 256 << 20
+
+WORKLOADS = {
+    # name: (variant, shape, algorithm, beta, init, seed, sweeps per step, bytes/update)
+    "msc16384": ("msc", (16384, 16384), "metropolis", BETA_C_2D, "hot", 7, 1000, 0.375),
+    "int8_1024": ("int8", (1024, 1024), "metropolis", BETA_C_2D, "hot", 1, 1000, 3.0),
+    "int8_3d_256": ("int8", (256, 256, 256), "heatbath", BETA_3D, "cold", 0, 2000, 3.0),
+}
+DESCRIPTION = {
+    "msc16384": "msc 2D Metropolis L=16384 (16384x128 u64 words per colour), periodic, T=T_c, "
+                "hot start seed 7, 1000 sweeps per step",
+    "int8_1024": "int8 2D Metropolis L=1024 compressed checkerboard, beta_c, hot start seed 1, "
+                 "1000 sweeps per step",
+    "int8_3d_256": "int8 3D heat bath L=256, beta=0.221654626, cold start, 2000 sweeps per step "
+                   "with (E, M) every 10 sweeps",
+}
+MEASURE_EVERY = {"int8_3d_256": 10}
+KERNEL = {"msc": "msc_half_kernel", "int8": "int8_half_kernel"}
+
+
+# ------------------------------------------------------------------------- helpers -------
+def dist_env() -> tuple[int, int, int]:
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic(kernel: str, workload: str) -> float | None:
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary, if there is one."""
+    p = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch"):
+            try:
+                return float(line.split("=")[1].split()[0])
+            except (IndexError, ValueError):
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self) -> None:
+        for line in self.proc.stdout:  # type: ignore[union-attr]
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc) -> None:
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9], strict=False):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "power_w_max": max(power) if power else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------ B200 arm -------
+def make_sim(wl: str, seed_offset: int = 0):
+    from pyising_b200.backend import B200Int8, B200MultiSpin
+
+    variant, shape, alg, beta, init, seed, _, _ = WORKLOADS[wl]
+    cls = B200MultiSpin if variant == "msc" else B200Int8
+    return cls(shape, beta, seed=seed + seed_offset, algorithm=alg, init=init)
+
+
+def run_device(wl: str, steps: int, warmup: int, rank: int, world: int, local: int,
+               dist) -> dict:
+    """Device-resident timing: K steps, CUDA events on the launching stream, L2 flushed."""
+    import torch
+
+    variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
+    every = MEASURE_EVERY.get(wl, 0)
+    sim = make_sim(wl, rank)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    st0 = sim.state()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def step():
+        if every:
+            sim.sweep_measured(sweeps, every)
+        else:
+            sim.sweep(sweeps)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    # restart from the workload's own start so the timed steps are the job itself
+    sim.load_colour_arrays(st0["c0"], st0["c1"])
+    sim.t = 0
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                events[i][0].record(stream)
+            step()
+            with torch.cuda.stream(stream):
+                events[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = sum(ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    n = int(np.prod(shape))
+    flips = n * sweeps * steps * world
+    value = flips / (total_ms * 1e6)
+    launches = 2 * sweeps * steps
+    avg_launch_ms = total_ms / launches
+    M, E = sim.observables_int()
+    out = {"value": value, "ms_per_step": total_ms / steps, "step_ms": ms,
+           "launches": launches, "avg_launch_ms": avg_launch_ms, "flips_per_step": n * sweeps,
+           "final_M": M, "final_E": E, "clocks": clk.summary(), "n_spins": n,
+           "bytes_per_update": bpu, "sim": sim}
+    del flush
+    return out
+
+
+def run_e2e(wl: str, steps: int, rank: int, world: int, dist) -> dict:
+    """The same job through the public API with host buffers: upload the start configuration,
+    sweep, download the final colour arrays and read (M, E), every step."""
+    import torch
+
+    variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
+    every = MEASURE_EVERY.get(wl, 0)
+    sim = make_sim(wl, rank)
+    st0 = sim.state()
+    c0, c1 = st0["c0"], st0["c1"]
+    h2d = c0.nbytes + c1.nbytes + sim.table.nbytes
+    d2h = c0.nbytes + c1.nbytes + 16 + (sweeps // every) * 16 if every else c0.nbytes + c1.nbytes + 16
+    sim.sweep(2)
+    sim.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.load_colour_arrays(c0, c1)
+        sim.t = 0
+        sim._upload_table()
+        if every:
+            sim.sweep_measured(sweeps, every)
+        else:
+            sim.sweep(sweeps)
+        sim.colour_arrays()
+        sim.observables_int()
+    sim.synchronize()
+    dt = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    n = int(np.prod(shape))
+    return {"value": n * sweeps * steps * world / (dt * 1e9), "unit": "flips/ns",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": dt * 1e3 / steps}
+
+
+def rng_ceiling(sim, variant: str) -> dict:
+    from pyising_b200._lib import philox_rate
+
+    rate = philox_rate(sim.device, 512, 5)
+    if variant == "msc":
+        mean = sim.philox_calls_per_word(2)
+        wmax = sim.philox_calls_per_word(2, warp=True)
+        calls_per_update = mean / 64.0
+        return {"philox_calls_per_ns": rate, "calls_per_word_mean": mean,
+                "calls_per_word_warp_max": wmax, "calls_per_update": calls_per_update,
+                "ceiling_flips_per_ns": rate / calls_per_update,
+                "ceiling_warp_max_flips_per_ns": rate / (wmax / 64.0)}
+    return {"philox_calls_per_ns": rate, "calls_per_update": 0.25,
+            "ceiling_flips_per_ns": rate / 0.25}
+
+
+def cpu_baseline(wl: str, budget_s: float = 10.0) -> dict:
+    """The oracle (the reference's algorithm in C, all host threads) on a bounded sample."""
+    import oracle
+
+    variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
+    cores = oracle.cpu_count()
+    oracle.set_threads(cores)
+    sim = oracle.create(variant, shape=shape, beta=beta, seed=seed, algorithm=alg, init=init)
+    t0 = time.perf_counter()
+    sim.sweep(1)
+    one = max(time.perf_counter() - t0, 1e-6)
+    n = max(1, min(sweeps, int(budget_s / one)))
+    t0 = time.perf_counter()
+    sim.sweep(n)
+    dt = time.perf_counter() - t0
+    rate = int(np.prod(shape)) * n / (dt * 1e9)
+    return {"value": rate, "unit": "flips/ns", "cores": cores, "kind": "port",
+            "sample": f"{n} sweeps of the same lattice (shape {list(shape)}, {variant}, "
+                      f"{alg}) on the C oracle, {cores} threads, {dt:.1f} s"}
+
+
+def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
+    import torch
+
+    wl = args.workload
+    variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
+    dev = run_device(wl, args.steps, args.warmup, rank, world, local, dist)
+    sim = dev.pop("sim")
+    e2e = run_e2e(wl, max(1, min(args.steps, 3)), rank, world, dist)
+    if rank != 0:
+        return None
+    peaks = measured_peaks()
+    n = dev["n_spins"]
+    bytes_per_launch = bpu * n / 2  # one colour = half the spins per launch
+    achieved = bytes_per_launch / (dev["avg_launch_ms"] * 1e-3) / 1e9
+    traffic = profile_traffic(KERNEL[variant], wl)
+    rng = rng_ceiling(sim, variant)
+    hbm_ceiling = peaks["hbm_gbs"] / bpu
+    line = {
+        "metric": "flips/ns", "value": round(dev["value"], 2), "unit": "flips/ns",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dev["ms_per_step"], 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64" if variant == "msc" else "int8",
+        "data": "synthetic (seeded hot/cold start; no dataset)",
+        "config": {"workload": DESCRIPTION[wl], "variant": variant, "shape": list(shape),
+                   "algorithm": alg, "beta": beta, "sweeps_per_step": sweeps,
+                   "l2": "flushed between steps (256 MiB write); the lattice stays "
+                         "L2-resident within a step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "pct_hbm_roofline": round(100 * dev["value"] / hbm_ceiling, 2),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4),
+                     "traffic": traffic,
+                     "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": KERNEL[variant],
+                     "bytes_per_launch": bytes_per_launch,
+                     "avg_launch_ms": round(dev["avg_launch_ms"], 5)},
+        "rng_roofline": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in rng.items()},
+        "e2e": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in e2e.items()},
+        "gpu_launches": dev["launches"],
+        "clocks": dev["clocks"],
+        "final_M_E": [dev["final_M"], dev["final_E"]],
+    }
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, args.cpu_budget)
+        line["cpu_baseline"]["value"] = round(line["cpu_baseline"]["value"], 4)
+    if args.extras and world == 1:
+        extras = {}
+        for other in WORKLOADS:
+            if other == wl:
+                continue
+            d = run_device(other, 3, 3, 0, 1, local, None)
+            d.pop("sim")
+            v, _, _, _, _, _, sw, b = WORKLOADS[other]
+            extras[other] = {"flips_per_ns": round(d["value"], 2),
+                             "ms_per_step": round(d["ms_per_step"], 4),
+                             "pct_hbm_roofline": round(100 * d["value"] * b / peaks["hbm_gbs"], 2),
+                             "description": DESCRIPTION[other]}
+        line["other_configs"] = extras
+    torch.cuda.synchronize()
+    return line
+
+
+def main_reference(args, rank: int) -> dict | None:
+    """The reference's algorithm on the host cores (the oracle port), one bounded sample per
+    step; rank 0 only."""
+    if rank != 0:
+        return None
+    import oracle
+
+    wl = args.workload
+    variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
+    cores = oracle.cpu_count()
+    oracle.set_threads(cores)
+    sim = oracle.create(variant, shape=shape, beta=beta, seed=seed, algorithm=alg, init=init)
+    t0 = time.perf_counter()
+    sim.sweep(1)
+    one = max(time.perf_counter() - t0, 1e-6)
+    per_step = max(1, min(sweeps, int(args.ref_step_s / one)))
+    for _ in range(args.warmup):
+        sim.sweep(per_step)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sim.sweep(per_step)
+        times.append(time.perf_counter() - t0)
+    n = int(np.prod(shape))
+    value = n * per_step * len(times) / (sum(times) * 1e9)
+    sample = (f"{per_step} sweeps per step of the {variant} lattice {list(shape)} ({alg}) on the "
+              f"C restatement of the reference algorithm, {cores} threads")
+    return {"impl": "reference", "metric": "flips/ns", "value": round(value, 4),
+            "unit": "flips/ns", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * sum(times) / len(times), 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64" if variant == "msc" else "int8", "data": "synthetic",
+            "config": {"workload": DESCRIPTION[wl], "variant": variant, "shape": list(shape),
+                       "sweeps_per_step": per_step},
+            "cpu_baseline": {"value": round(value, 4), "unit": "flips/ns", "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "flips/ns", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="msc16384")
+    ap.add_argument("--no-extras", dest="extras", action="store_false")
+    ap.add_argument("--cpu-budget", type=float, default=10.0,
+                    help="seconds of oracle work for cpu_baseline")
+    ap.add_argument("--ref-step-s", type=float, default=2.0,
+                    help="seconds of oracle work per step of --impl reference")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        line = main_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    torch.cuda.set_device(local)
+    os.environ["PYISING_B200_DEVICE"] = str(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local))
+        dist = td
+    try:
+        line = main_b200(args, rank, world, local, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,35 @@
+"""Run one small sweep case, for profilers (ncu) and quick timing.
+
+    python -m pyising_b200.profile_case {int8|hb3|msc} L SWEEPS
+
+int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
+beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7.
+Prints the final exact (M, E).
+"""
+
+from __future__ import annotations
+
+import sys
+
+from .backend import B200Int8, B200MultiSpin
+from .lattice import BETA_C_2D
+
+
+def main(argv: list[str]) -> int:
+    which, L, n = argv[0], int(argv[1]), int(argv[2])
+    if which == "int8":
+        sim = B200Int8((L, L), BETA_C_2D, seed=7, init="hot")
+    elif which == "hb3":
+        sim = B200Int8((L, L, L), 0.221654626, seed=0, algorithm="heatbath", init="cold")
+    elif which == "msc":
+        sim = B200MultiSpin((L, L), BETA_C_2D, seed=7, init="hot")
+    else:
+        raise SystemExit(f"unknown case {which!r}")
+    sim.sweep(n)
+    sim.synchronize()
+    print(which, L, n, sim.observables_int())
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main(sys.argv[1:]))
