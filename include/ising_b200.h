@@ -124,6 +124,25 @@ int ising_device_bytes(ising_sim* h, int64_t* bytes);
 int ising_msc_calls_per_word(ising_sim* h, uint64_t t0, int64_t n_sweeps, double* mean,
                              double* warp_max);
 
+/* Sweeps on caller-owned device arrays that allocate nothing.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc (device memory owned by a pool they do not
+ * control, or a loop that must not take cudaMalloc/cudaFree's implicit synchronisation).
+ * c0, c1: the two colour arrays in device memory, laid out as ising_upload expects (int8
+ * (rows, Lx/2) or packed uint64 (rows, Lx/128)), 16-byte aligned, updated in place.  Arguments
+ * otherwise as ising_create + ising_set_table + ising_sweep; the work runs on `stream`
+ * (cudaStream_t, NULL = default stream) on the calling thread's current device.
+ * Measured (M, E) sums live in a fixed 64 KiB device array inside the library (held by every
+ * GPU that loads it until exit): at most 4096 measurements (n_sweeps / measure_every) per call,
+ * more is rejected with ISING_ERR_INVALID.  The first call on a device looks the array's address
+ * up (cudaGetSymbolAddress); make that first call before any stream capture.  Every call shares
+ * the array, so calls that overlap on the GPU (other streams, other threads) race; the
+ * measured part is cleared at the start of each call.  Blocks until series_out is written when
+ * measure_every > 0, otherwise only enqueues the work. */
+int ising_sweep_static(int ndim, const int64_t* shape, int variant, int algorithm, uint64_t seed,
+                       const uint32_t* table, int table_n, void* c0, void* c1, uint64_t t0,
+                       int64_t n_sweeps, int64_t measure_every, int64_t* series_out,
+                       void* stream);
+
 /* ---- device probes (roofline ceilings and generator checks) ---------------------------- */
 
 /* Philox4x32-10 throughput of this device in calls/ns (best of `repeats`).

@@ -45,6 +45,7 @@ SIGNATURES: dict[str, tuple] = {
     "ising_sync": (I, [P]),
     "ising_device_bytes": (I, [P, PI64]),
     "ising_msc_calls_per_word": (I, [P, U64, I64, PD, PD]),
+    "ising_sweep_static": (I, [I, PI64, I, I, U64, P, I, P, P, U64, I64, I64, P, P]),
     "ising_philox_rate": (I, [I, I, I, PD]),
     "ising_philox_range": (I, [I, U32, I64, U32, U32, U32, U32, U32, P]),
 }
