@@ -160,6 +160,11 @@ int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uin
         ising_destroy(h);
         return fail(ISING_ERR_NOMEM, "cudaMalloc of the accumulators failed");
     }
+    e = cudaMemset(h->d_acc, 0, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        ising_destroy(h);
+        return cuda_fail(e, "cudaMemset of the accumulators");
+    }
     *out = h;
     return ISING_OK;
 }

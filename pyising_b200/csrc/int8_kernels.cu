@@ -137,7 +137,7 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
 }
 
 template <int V, int NDIM, int RULE>
-__global__ void __launch_bounds__(256) int8_half_kernel(const Int8Half p)
+__global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
 {
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
@@ -145,12 +145,29 @@ __global__ void __launch_bounds__(256) int8_half_kernel(const Int8Half p)
     long long m_acc = 0, e_acc = 0;
     if (jc < p.cpr) {
         const int j0 = jc * V;
-        const long long row_step = (long long)gridDim.y * blockDim.y;
-        for (long long row = (long long)blockIdx.y * blockDim.y + threadIdx.y; row < p.rows;
-             row += row_step) {
-            const int r32 = (int)row;
-            const int y = r32 % p.ly;
-            const int z = r32 / p.ly;
+        const int row_step = gridDim.y * blockDim.y;
+        const int row0 = blockIdx.y * blockDim.y + threadIdx.y;
+        // (y, z) of the row, advanced without divisions in the loop (rows < 2^31)
+        int y = row0, z = 0, sy = row_step, sz = 0;
+        if constexpr (NDIM == 3) {
+            z = row0 / p.ly;
+            y = row0 - z * p.ly;
+            sz = row_step / p.ly;
+            sy = row_step - sz * p.ly;
+        }
+        for (long long row = row0; row < p.rows; row += row_step) {
+            if constexpr (NDIM == 3) {
+                if (row != row0) {
+                    y += sy;
+                    z += sz;
+                    if (y >= p.ly) {
+                        y -= p.ly;
+                        ++z;
+                    }
+                }
+            } else {
+                y = (int)row;
+            }
             const int par = (y + z + (int)p.color) & 1;
             const long long rb = row * p.lh;
             const int8_t* orow = p.other + rb;
