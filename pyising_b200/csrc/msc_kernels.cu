@@ -105,17 +105,23 @@ __global__ void __launch_bounds__(256) msc_half_kernel(const MscHalf p)
 // at T_c, but 6.3 for the slowest word of a warp), so a one-word-per-lane kernel idles most
 // lanes in its last iterations.  Here:
 //   * intake: a warp takes the next 32 words of its contiguous range (their global loads were
-//     issued when the previous batch was consumed), bit-slices them and draws three Philox
-//     blocks per word unconditionally (at T_c 95% of words need three or more); decided words
+//     issued when the previous batch was consumed), bit-slices them and draws four Philox
+//     blocks per word unconditionally (at T_c half of the words need four or more); decided words
 //     are stored, the others pushed on the warp's 64-entry stack in shared memory;
 //   * while the stack holds 32 or more entries (or no words are left): pop up to 32, draw one
 //     Philox block each at the entry's own level pair, store finished words, push back the rest.
 // The random numbers, bit levels and their order are the reference's; only the schedule
 // differs, so results are identical.  Lanes are handled as two independent 32-bit halves.
 
+#ifndef ISING_MSC_INTAKE_CALLS
+#define ISING_MSC_INTAKE_CALLS 4
+#endif
+#ifndef ISING_MSC_MIN_BLOCKS
+#define ISING_MSC_MIN_BLOCKS 1
+#endif
 constexpr int kQueueWarps = 8;
 constexpr int kQueueCap = 64;
-constexpr int kIntakeCalls = 3;
+constexpr int kIntakeCalls = ISING_MSC_INTAKE_CALLS;  // Philox blocks per word before queueing
 
 struct QueueSlots {
     u32 idx[kQueueCap];
@@ -173,7 +179,7 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
     L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
 }
 
-__global__ void __launch_bounds__(kQueueWarps * 32)
+__global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
     msc_half_queue_kernel(const MscHalf p, long long total, long long per_warp, int nw_shift)
 {
     __shared__ QueueSlots q_all[kQueueWarps];
