@@ -143,6 +143,76 @@ int ising_sweep_static(int ndim, const int64_t* shape, int variant, int algorith
                        int64_t n_sweeps, int64_t measure_every, int64_t* series_out,
                        void* stream);
 
+/* Device-side seeded start (not in the reference, whose hot start is NumPy's PCG64 and stays
+ * the default of the Python layer): compressed site n of colour c is +1 iff bit n % 32 of word
+ * (n / 32) % 4 of Philox4x32-10((n / 128, 0, c, 0xFFFFFFFF), start_seed) is set.  The same
+ * spins for the int8 and the packed layout; no host work, so multi-GB starts cost a kernel. */
+int ising_fill_philox(ising_sim* h, uint64_t start_seed);
+
+/* ---- batched ensembles and serving ----------------------------------------------------- */
+/* No counterpart in the reference (which runs one lattice per launch): many independent
+ * lattices of uneven size, dimension, variant and temperature advance together, one grouped
+ * launch per half-sweep over a (lattice, tile) work list; each lattice stays bit-identical to
+ * running it alone (the random numbers depend only on site, sweep, colour and seed). */
+
+#define ISING_INIT_COLD 0     /* all +1 */
+#define ISING_INIT_PHILOX 1   /* the device seeded start of ising_fill_philox, seed = job seed */
+#define ISING_INIT_LATTICE 2  /* a full int8 lattice, copied when the job is added */
+
+#define ISING_JOB_PENDING 0   /* waiting for memory (admission at the next sweep boundary) */
+#define ISING_JOB_ACTIVE 1
+#define ISING_JOB_FINISHING 2 /* last sweep issued, results on their way to the host */
+#define ISING_JOB_DONE 3
+
+typedef struct ising_job {
+    int ndim;                 /* 2 or 3 */
+    int64_t shape[3];         /* (Ly, Lx) or (Lz, Ly, Lx) */
+    int variant;              /* ISING_VARIANT_* */
+    int algorithm;            /* ISING_METROPOLIS / ISING_HEATBATH */
+    uint64_t seed;            /* Philox key */
+    uint32_t table[7];        /* threshold_table(beta, ndim, algorithm) */
+    int table_n;              /* 2 * ndim + 1 */
+    uint64_t t0;              /* sweep counter of the first sweep */
+    int64_t n_sweeps;
+    int64_t measure_every;    /* (M, E) after every measure_every-th sweep; 0 = none */
+    int init;                 /* ISING_INIT_* */
+    const int8_t* lattice;    /* ISING_INIT_LATTICE: full lattice, C order (copied) */
+    int keep_lattice;         /* non-zero: copy the final lattice back for *_result */
+} ising_job;
+
+typedef struct ising_batch ising_batch;
+
+/* A batch on `device` whose lattices and series may hold at most memory_budget device bytes.
+ * Replaces running lattices one at a time through create()/sweep() (bench/run.py:121-142). */
+int ising_batch_create(int device, int64_t memory_budget, ising_batch** out);
+/* Queue a job (validated like ising_create); it joins at the next sweep boundary with room. */
+int ising_batch_add(ising_batch* b, const ising_job* job, int64_t* id);
+/* Advance every job until all are done (max_epochs <= 0) or for max_epochs half-sweeps. */
+int ising_batch_run(ising_batch* b, int64_t max_epochs, int64_t* epochs_run);
+int ising_batch_status(ising_batch* b, int64_t id, int* state, int64_t* sweeps_done);
+/* Results of a done job: series (n_sweeps / measure_every pairs of (M, E)), final lattice. */
+int ising_batch_result(ising_batch* b, int64_t id, int64_t* series_out, int8_t* lattice_out);
+int ising_batch_release(ising_batch* b, int64_t id);
+int ising_batch_destroy(ising_batch* b);
+
+typedef struct ising_server ising_server;
+
+/* A serving loop on its own host thread: submitted jobs are admitted by the memory budget at
+ * sweep boundaries while others run (continuous batching), results stay on the host until
+ * released.  Submit, wait, result, status and release are thread-safe. */
+int ising_server_create(int device, int64_t memory_budget, ising_server** out);
+int ising_server_submit(ising_server* s, const ising_job* job, int64_t* id);
+/* Wait up to timeout_s seconds (< 0: no limit) for the job; *state is its ISING_JOB_* state. */
+int ising_server_wait(ising_server* s, int64_t id, double timeout_s, int* state);
+/* Results of a done job and its submit-to-done latency in seconds. */
+int ising_server_result(ising_server* s, int64_t id, int64_t* series_out, int8_t* lattice_out,
+                        double* latency_s);
+int ising_server_release(ising_server* s, int64_t id);
+int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int64_t* used_bytes,
+                        int64_t* epoch);
+/* Finish the jobs already submitted, stop the thread and free everything. */
+int ising_server_destroy(ising_server* s);
+
 /* ---- device probes (roofline ceilings and generator checks) ---------------------------- */
 
 /* Philox4x32-10 throughput of this device in calls/ns (best of `repeats`).

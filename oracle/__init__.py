@@ -192,6 +192,24 @@ def energy_magnetization(lat: np.ndarray) -> tuple[int, int]:
     return int(lat64.sum()), e
 
 
+def philox_start(shape, seed: int) -> np.ndarray:
+    """The device seeded start of the product (``init="philox"``; not part of the reference):
+    compressed site n of colour c is +1 iff bit n % 32 of word (n // 32) % 4 of
+    Philox((n // 128, 0, c, 0xFFFFFFFF), seed) is set.  Returns the full lattice."""
+    shape = tuple(int(s) for s in shape)
+    rows = int(np.prod(shape[:-1]))
+    sites = rows * shape[-1] // 2
+    groups = (sites + 127) // 128
+    k0, k1 = split_seed(seed)
+    cols = []
+    for c in (0, 1):
+        r = philox_range(0, groups, 0, c, 0xFFFFFFFF, k0, k1)  # (groups, 4) uint32
+        bits = np.unpackbits(r.astype("<u4").view(np.uint8).reshape(groups, 16), axis=1,
+                             bitorder="little").reshape(-1)[:sites]
+        cols.append((bits.astype(np.int8) * 2 - 1).reshape(rows, shape[-1] // 2))
+    return from_compressed(cols[0], cols[1], shape)
+
+
 # --------------------------------------------------------------- simulations -------------
 def _shape_arr(shape) -> np.ndarray:
     return np.asarray(list(shape) + [0] * (3 - len(shape)), dtype=np.int64)

@@ -46,6 +46,21 @@ SIGNATURES: dict[str, tuple] = {
     "ising_device_bytes": (I, [P, PI64]),
     "ising_msc_calls_per_word": (I, [P, U64, I64, PD, PD]),
     "ising_sweep_static": (I, [I, PI64, I, I, U64, P, I, P, P, U64, I64, I64, P, P]),
+    "ising_fill_philox": (I, [P, U64]),
+    "ising_batch_create": (I, [I, I64, ctypes.POINTER(P)]),
+    "ising_batch_add": (I, [P, P, PI64]),
+    "ising_batch_run": (I, [P, I64, PI64]),
+    "ising_batch_status": (I, [P, I64, ctypes.POINTER(I), PI64]),
+    "ising_batch_result": (I, [P, I64, P, P]),
+    "ising_batch_release": (I, [P, I64]),
+    "ising_batch_destroy": (I, [P]),
+    "ising_server_create": (I, [I, I64, ctypes.POINTER(P)]),
+    "ising_server_submit": (I, [P, P, PI64]),
+    "ising_server_wait": (I, [P, I64, ctypes.c_double, ctypes.POINTER(I)]),
+    "ising_server_result": (I, [P, I64, P, P, PD]),
+    "ising_server_release": (I, [P, I64]),
+    "ising_server_status": (I, [P, PI64, PI64, PI64, PI64]),
+    "ising_server_destroy": (I, [P]),
     "ising_philox_rate": (I, [I, I, I, PD]),
     "ising_philox_range": (I, [I, U32, I64, U32, U32, U32, U32, U32, P]),
 }

@@ -59,6 +59,11 @@ class _B200Simulation(IsingSimulation):
     def _fill_cold(self) -> None:
         check(lib().ising_fill_cold(self._h), "fill_cold")
 
+    def _fill_philox(self) -> None:
+        """``init="philox"``: the device seeded start of ``ising_fill_philox`` keyed by the
+        simulation's seed (no host work; not pyising's NumPy hot start)."""
+        check(lib().ising_fill_philox(self._h, self.seed), "fill_philox")
+
     def set_lattice(self, lat: np.ndarray) -> None:
         full = np.ascontiguousarray(np.asarray(lat, dtype=np.int8).reshape(self.shape))
         check(lib().ising_set_lattice(self._h, full.ctypes.data), "set_lattice")

@@ -55,6 +55,8 @@ class IsingSimulation(ABC):
             self._fill_cold()
         elif init == "hot":
             self._fill_hot()
+        elif init == "philox":
+            self._fill_philox()
         else:
             raise ValueError(f"unknown init {init!r}")
 
@@ -95,6 +97,9 @@ class IsingSimulation(ABC):
 
     def _fill_cold(self) -> None:
         self.set_lattice(np.ones(self.shape, dtype=np.int8))
+
+    def _fill_philox(self) -> None:
+        raise ValueError(f"{self.backend}/{self.variant} has no device seeded start")
 
     def synchronize(self) -> None:  # noqa: B027 - optional hook
         pass

@@ -1,0 +1,923 @@
+// Batched ensembles and continuous-batching serving: many independent lattices of uneven size,
+// dimension, variant and temperature advanced together, one grouped launch per half-sweep
+// "epoch" over a (lattice, tile) work list.
+//
+// Every lattice keeps its own seed, table, sweep counter and measurement interval.  Its sweep
+// counter at epoch e is t0 + (e - join) / 2 (lattices join at even epochs, so every launch
+// updates one colour, e % 2, of every active lattice); its (M, E) after sweep s lands in its
+// own series slot.  The random numbers depend only on (site, sweep, colour, seed), so each
+// lattice is bit-identical to running it alone with the single-lattice kernels.
+//
+// Work items are tiles of ~16K int8 sites (whole rows) or ~4K packed words; items of one
+// kernel class (variant, chunk width, dims, decision rule) share a launch; a block walks its
+// items grid-stride.  The host engine decides membership deterministically from sweep counts,
+// so it never waits for the device except to hand results back (events) and to bound how far
+// it runs ahead.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "capi_internal.h"
+#include "int8_core.cuh"
+#include "msc_core.cuh"
+
+namespace ising {
+
+struct BatchLattice {
+    void* c[2];
+    long long* series;     // (M, E) pairs, or nullptr
+    long long join_epoch;  // even epoch of the first half-sweep
+    int variant;
+    int ndim;
+    int rows, lh, ly, lz, cpr, nw, nw_shift;
+    int bx_log2;           // int8: threads along a row = 1 << bx_log2 (of 256)
+    int every;             // measurement interval in sweeps (0 = none)
+    u32 t0;
+    u32 k0, k1;
+    u32 table[7];
+};
+
+struct BatchItem {
+    int lat;
+    int pad;
+    long long begin, end;  // rows (int8) or words (msc)
+};
+
+template <int V, int NDIM, int RULE>
+__global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* __restrict__ lats,
+                                                         const BatchItem* __restrict__ items,
+                                                         int n_items, long long epoch)
+{
+    const u32 color = (u32)(epoch & 1);
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BatchItem item = items[it];
+        const BatchLattice& L = lats[item.lat];
+        const long long s = (epoch - L.join_epoch) >> 1;
+        const bool meas = color == 1 && L.every > 0 && ((s + 1) % L.every) == 0;
+        Int8Half p;
+        p.own = static_cast<int8_t*>(L.c[color]);
+        p.other = static_cast<const int8_t*>(L.c[color ^ 1]);
+        p.rows = L.rows;
+        p.lh = L.lh;
+        p.ly = L.ly;
+        p.lz = L.lz;
+        p.cpr = L.cpr;
+        p.t = L.t0 + (u32)s;
+        p.color = color;
+        p.k0 = L.k0;
+        p.k1 = L.k1;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) p.table[i] = L.table[i];
+        p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
+                      : nullptr;
+        const int bx = 1 << L.bx_log2;
+        const int tx = threadIdx.x & (bx - 1), ty = threadIdx.x >> L.bx_log2;
+        const int by = 256 >> L.bx_log2;
+        long long m_acc = 0, e_acc = 0;
+        for (long long row = item.begin + ty; row < item.end; row += by) {
+            int y = (int)row, z = 0;
+            if constexpr (NDIM == 3) {
+                z = (int)(row / L.ly);
+                y = (int)(row - (long long)z * L.ly);
+            }
+            for (int jc = tx; jc < p.cpr; jc += bx)
+                int8_chunk<V, NDIM, RULE>(p, row, y, z, jc * V, m_acc, e_acc);
+        }
+        if (meas) block_accumulate2(m_acc, e_acc, p.meas);
+        __syncthreads();
+    }
+}
+
+constexpr int kBatchWarps = 8;
+
+__global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
+    const BatchLattice* __restrict__ lats, const BatchItem* __restrict__ items, int n_items,
+    long long epoch)
+{
+    __shared__ QueueSlots q_all[kBatchWarps];
+    __shared__ uint4 lvmask[16];
+    const u32 color = (u32)(epoch & 1);
+    const int warp = threadIdx.x >> 5;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BatchItem item = items[it];
+        const BatchLattice& L = lats[item.lat];
+        const long long s = (epoch - L.join_epoch) >> 1;
+        const bool meas = color == 1 && L.every > 0 && ((s + 1) % L.every) == 0;
+        MscHalf p;
+        p.own = static_cast<u64*>(L.c[color]);
+        p.other = static_cast<const u64*>(L.c[color ^ 1]);
+        p.rows = L.rows;
+        p.nw = L.nw;
+        p.t = L.t0 + (u32)s;
+        p.color = color;
+        p.k0 = L.k0;
+        p.k1 = L.k1;
+        p.thr4 = L.table[3];
+        p.thr8 = L.table[4];
+        p.stats = nullptr;
+        p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
+                      : nullptr;
+        if (meas) {
+            long long m_acc = 0, e_acc = 0, ca = 0, wm = 0;
+            for (long long w = item.begin + threadIdx.x; w < item.end; w += blockDim.x) {
+                const int y = (int)(L.nw_shift >= 0 ? (w >> L.nw_shift) : (w / L.nw));
+                msc_word<true>(p, y, (int)(w - (long long)y * L.nw), m_acc, e_acc, ca, wm);
+            }
+            block_accumulate2(m_acc, e_acc, p.meas);
+        } else {
+            if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+            __syncthreads();
+            const long long len = item.end - item.begin;
+            long long per = (len + kBatchWarps - 1) / kBatchWarps;
+            per = (per + 31) / 32 * 32;
+            const long long b = item.begin + warp * per;
+            const long long e = min(b + per, item.end);
+            msc_queue_range(p, b, e, L.nw_shift, q_all[warp], lvmask);
+        }
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------------------------- host engine ---
+cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
+                                int max_blocks, cudaStream_t st);
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+    int64_t id = 0;
+    int state = ISING_JOB_PENDING;
+    ising_job spec;
+    std::vector<int8_t> init;  // host copy of an initial lattice (ISING_INIT_LATTICE)
+    int rows = 0, lh = 0, ly = 0, lz = 1, nw = 0;
+    size_t colour_bytes = 0, series_pairs = 0, device_bytes = 0;
+    void* c[2] = {nullptr, nullptr};
+    long long* d_series = nullptr;
+    long long* h_series = nullptr;  // pinned
+    int8_t* h_lattice = nullptr;    // pinned, keep_lattice only
+    long long join_epoch = -1;
+    cudaEvent_t done_event = nullptr;
+    Clock::time_point t_submit, t_start, t_done;
+    std::string error;
+};
+
+struct KernelClass {
+    int variant, v, ndim, rule;
+    bool operator<(const KernelClass& o) const
+    {
+        return std::tie(variant, v, ndim, rule) < std::tie(o.variant, o.v, o.ndim, o.rule);
+    }
+};
+
+class Engine {
+public:
+    Engine(int device, int64_t budget) : device_(device), budget_(budget) {}
+
+    int init()
+    {
+        cudaError_t e = cudaSetDevice(device_);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+        e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+        sms_ = device_sm_count(device_);
+        return ISING_OK;
+    }
+
+    ~Engine()
+    {
+        cudaSetDevice(device_);
+        if (stream_) cudaStreamSynchronize(stream_);
+        for (auto& kv : jobs_) free_job(*kv.second, true);
+        if (d_lats_) cudaFree(d_lats_);
+        if (d_items_) cudaFree(d_items_);
+        for (cudaEvent_t ev : epoch_events_) cudaEventDestroy(ev);
+        if (stream_) cudaStreamDestroy(stream_);
+        cudaGetLastError();
+    }
+
+    // Validates the job and queues it; returns its id.
+    int submit(const ising_job& spec, int64_t* id)
+    {
+        auto j = std::make_unique<Job>();
+        int rc = validate(spec, *j);
+        if (rc != ISING_OK) return rc;
+        j->spec = spec;
+        if (spec.init == ISING_INIT_LATTICE) {
+            const size_t n = (size_t)j->rows * 2 * j->lh;
+            j->init.assign(spec.lattice, spec.lattice + n);
+        }
+        j->spec.lattice = nullptr;
+        if ((int64_t)j->device_bytes > budget_)
+            return fail(ISING_ERR_NOMEM, "job needs %zu device bytes, over the %lld-byte budget",
+                        j->device_bytes, (long long)budget_);
+        j->id = ++last_id_;
+        j->t_submit = Clock::now();
+        *id = j->id;
+        pending_.push_back(j->id);
+        jobs_[j->id] = std::move(j);
+        return ISING_OK;
+    }
+
+    bool busy() const { return !active_.empty() || !pending_.empty() || !finishing_.empty(); }
+    bool has_work() const { return !active_.empty() || !pending_.empty(); }
+    size_t active_count() const { return active_.size(); }
+    size_t pending_count() const { return pending_.size(); }
+    long long epoch() const { return epoch_; }
+    int64_t used_bytes() const { return used_; }
+
+    // One half-sweep of every active lattice (admitting pending jobs at even epochs).
+    int step()
+    {
+        cudaError_t e = cudaSetDevice(device_);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+        if ((epoch_ & 1) == 0) {
+            int rc = admit();
+            if (rc != ISING_OK) return rc;
+        }
+        if (active_.empty()) return ISING_OK;
+        if (dirty_) {
+            int rc = rebuild();
+            if (rc != ISING_OK) return rc;
+        }
+        for (const auto& cl : classes_) {
+            e = launch_class(cl.first, cl.second.first, cl.second.second);
+            if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+        }
+        ++epoch_;
+        if ((epoch_ & 1) == 0) {
+            int rc = retire();
+            if (rc != ISING_OK) return rc;
+            rc = throttle();
+            if (rc != ISING_OK) return rc;
+        }
+        return ISING_OK;
+    }
+
+    // Marks finished result copies as done; returns how many completed.
+    int poll()
+    {
+        int n = 0;
+        for (auto it = finishing_.begin(); it != finishing_.end();) {
+            Job& j = *jobs_[*it];
+            const cudaError_t e = cudaEventQuery(j.done_event);
+            if (e == cudaSuccess) {
+                j.state = ISING_JOB_DONE;
+                j.t_done = Clock::now();
+                cudaEventDestroy(j.done_event);
+                j.done_event = nullptr;
+                it = finishing_.erase(it);
+                ++n;
+            } else if (e == cudaErrorNotReady) {
+                ++it;
+            } else {
+                return cuda_fail(e, "result event");
+            }
+        }
+        return n;
+    }
+
+    int wait_finishing()
+    {
+        cudaError_t e = cudaStreamSynchronize(stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+        poll();
+        return ISING_OK;
+    }
+
+    Job* find(int64_t id)
+    {
+        auto it = jobs_.find(id);
+        return it == jobs_.end() ? nullptr : it->second.get();
+    }
+
+    int result(int64_t id, int64_t* series_out, int8_t* lattice_out, double* latency)
+    {
+        Job* j = find(id);
+        if (!j) return fail(ISING_ERR_INVALID, "unknown job %lld", (long long)id);
+        if (j->state != ISING_JOB_DONE)
+            return fail(ISING_ERR_STATE, "job %lld is not done", (long long)id);
+        if (series_out && j->series_pairs)
+            memcpy(series_out, j->h_series, j->series_pairs * 2 * sizeof(long long));
+        if (lattice_out) {
+            if (!j->h_lattice)
+                return fail(ISING_ERR_STATE, "job %lld was not submitted with keep_lattice",
+                            (long long)id);
+            memcpy(lattice_out, j->h_lattice, (size_t)j->rows * 2 * j->lh);
+        }
+        if (latency)
+            *latency = std::chrono::duration<double>(j->t_done - j->t_submit).count();
+        return ISING_OK;
+    }
+
+    int release(int64_t id)
+    {
+        auto it = jobs_.find(id);
+        if (it == jobs_.end()) return fail(ISING_ERR_INVALID, "unknown job %lld", (long long)id);
+        Job& j = *it->second;
+        if (j.state == ISING_JOB_ACTIVE || j.state == ISING_JOB_FINISHING)
+            return fail(ISING_ERR_STATE, "job %lld is still running", (long long)id);
+        if (j.state == ISING_JOB_PENDING)
+            pending_.erase(std::remove(pending_.begin(), pending_.end(), id), pending_.end());
+        free_job(j, false);
+        jobs_.erase(it);
+        return ISING_OK;
+    }
+
+    int64_t budget() const { return budget_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    int validate(const ising_job& s, Job& j)
+    {
+        if (s.ndim != 2 && s.ndim != 3)
+            return fail(ISING_ERR_INVALID, "only 2D and 3D lattices are supported");
+        for (int i = 0; i < s.ndim; ++i)
+            if (s.shape[i] < 2 || s.shape[i] % 2)
+                return fail(ISING_ERR_INVALID, "all extents must be even and >= 2");
+        if (s.variant != ISING_VARIANT_INT8 && s.variant != ISING_VARIANT_MSC)
+            return fail(ISING_ERR_INVALID, "unknown variant %d", s.variant);
+        if (s.algorithm != ISING_METROPOLIS && s.algorithm != ISING_HEATBATH)
+            return fail(ISING_ERR_INVALID, "unknown algorithm %d", s.algorithm);
+        if (s.variant == ISING_VARIANT_MSC && (s.ndim != 2 || s.algorithm != ISING_METROPOLIS))
+            return fail(ISING_ERR_INVALID, "msc supports 2D Metropolis only");
+        const int64_t lx = s.shape[s.ndim - 1];
+        if (lx % (s.variant == ISING_VARIANT_MSC ? 128 : 8))
+            return fail(ISING_ERR_INVALID, "last extent must be a multiple of %d",
+                        s.variant == ISING_VARIANT_MSC ? 128 : 8);
+        if (s.table_n != 2 * s.ndim + 1)
+            return fail(ISING_ERR_INVALID, "table must have %d entries", 2 * s.ndim + 1);
+        if (s.n_sweeps < 0 || s.measure_every < 0)
+            return fail(ISING_ERR_INVALID, "negative sweep count or interval");
+        if (s.init != ISING_INIT_COLD && s.init != ISING_INIT_PHILOX && s.init != ISING_INIT_LATTICE)
+            return fail(ISING_ERR_INVALID, "unknown init %d", s.init);
+        if (s.init == ISING_INIT_LATTICE && !s.lattice)
+            return fail(ISING_ERR_INVALID, "ISING_INIT_LATTICE needs a lattice");
+        const int64_t ly = s.shape[s.ndim - 2], lz = s.ndim == 3 ? s.shape[0] : 1;
+        if (ly * lz > 0x7FFFFFFF || lx / 2 > 0x7FFFFFFF)
+            return fail(ISING_ERR_INVALID, "lattice too large");
+        j.rows = (int)(ly * lz);
+        j.lh = (int)(lx / 2);
+        j.ly = (int)ly;
+        j.lz = (int)lz;
+        j.nw = (int)(lx / 128);
+        j.colour_bytes = s.variant == ISING_VARIANT_MSC ? (size_t)j.rows * j.nw * 8
+                                                       : (size_t)j.rows * j.lh;
+        j.series_pairs = s.measure_every > 0 ? (size_t)(s.n_sweeps / s.measure_every) : 0;
+        j.device_bytes = 2 * j.colour_bytes + j.series_pairs * 2 * sizeof(long long);
+        return ISING_OK;
+    }
+
+    int admit()
+    {
+        for (auto it = pending_.begin(); it != pending_.end();) {
+            Job& j = *jobs_[*it];
+            if (used_ + (int64_t)j.device_bytes > budget_) {
+                ++it;  // later, smaller jobs may still fit
+                continue;
+            }
+            int rc = start_job(j);
+            if (rc != ISING_OK) return rc;
+            it = pending_.erase(it);
+        }
+        return ISING_OK;
+    }
+
+    int start_job(Job& j)
+    {
+        cudaError_t e;
+        for (int c = 0; c < 2; ++c) {
+            e = cudaMallocAsync(&j.c[c], j.colour_bytes, stream_);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync (job lattice)");
+        }
+        if (j.series_pairs) {
+            const size_t sb = j.series_pairs * 2 * sizeof(long long);
+            e = cudaMallocAsync((void**)&j.d_series, sb, stream_);
+            if (e == cudaSuccess) e = cudaMemsetAsync(j.d_series, 0, sb, stream_);
+            if (e != cudaSuccess) return cuda_fail(e, "job series");
+        }
+        const ising_job& s = j.spec;
+        const int max_blocks = sms_ * 8;
+        if (s.init == ISING_INIT_COLD) {
+            const int v = s.variant == ISING_VARIANT_MSC ? 0xFF : 0x01;
+            for (int c = 0; c < 2 && e == cudaSuccess; ++c)
+                e = cudaMemsetAsync(j.c[c], v, j.colour_bytes, stream_);
+        } else if (s.init == ISING_INIT_PHILOX) {
+            e = launch_philox_start(j.c[0], j.c[1], (long long)j.rows * j.lh,
+                                    s.variant == ISING_VARIANT_MSC, (u32)s.seed,
+                                    (u32)(s.seed >> 32), max_blocks, stream_);
+        } else {
+            const size_t full = (size_t)j.rows * 2 * j.lh;
+            int8_t* stage = nullptr;
+            e = cudaMallocAsync((void**)&stage, full, stream_);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(stage, j.init.data(), full, cudaMemcpyHostToDevice, stream_);
+            if (e == cudaSuccess) {
+                if (s.variant == ISING_VARIANT_MSC)
+                    e = launch_msc_pack(stage, (u64*)j.c[0], (u64*)j.c[1], j.rows, 0, j.nw,
+                                        max_blocks, stream_);
+                else
+                    e = launch_int8_split(stage, (int8_t*)j.c[0], (int8_t*)j.c[1], j.rows, 0,
+                                          j.lh, j.ly, max_blocks, stream_);
+            }
+            if (stage) cudaFreeAsync(stage, stream_);
+            std::vector<int8_t>().swap(j.init);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "job start");
+        used_ += (int64_t)j.device_bytes;
+        j.join_epoch = epoch_;
+        j.state = ISING_JOB_ACTIVE;
+        j.t_start = Clock::now();
+        if (s.n_sweeps == 0) {
+            j.state = ISING_JOB_ACTIVE;
+            return finish_job(j);
+        }
+        active_.push_back(j.id);
+        dirty_ = true;
+        return ISING_OK;
+    }
+
+    // Builds the lattice table and the work items, grouped by kernel class.
+    int rebuild()
+    {
+        std::vector<BatchLattice> lats;
+        std::map<KernelClass, std::vector<BatchItem>> by_class;
+        lats.reserve(active_.size());
+        for (int64_t id : active_) {
+            Job& j = *jobs_[id];
+            const ising_job& s = j.spec;
+            BatchLattice L;
+            memset(&L, 0, sizeof L);
+            L.c[0] = j.c[0];
+            L.c[1] = j.c[1];
+            L.series = j.d_series;
+            L.join_epoch = j.join_epoch;
+            L.variant = s.variant;
+            L.ndim = s.ndim;
+            L.rows = j.rows;
+            L.lh = j.lh;
+            L.ly = j.ly;
+            L.lz = j.lz;
+            L.nw = j.nw;
+            L.nw_shift = s.variant == ISING_VARIANT_MSC && (j.nw & (j.nw - 1)) == 0
+                             ? __builtin_ctz((unsigned)j.nw) : -1;
+            L.every = (int)s.measure_every;
+            L.t0 = (u32)s.t0;
+            L.k0 = (u32)s.seed;
+            L.k1 = (u32)(s.seed >> 32);
+            for (int i = 0; i < 7; ++i) L.table[i] = i < s.table_n ? s.table[i] : 0xFFFFFFFFu;
+            KernelClass kc{s.variant, 0, s.ndim, 0};
+            const int li = (int)lats.size();
+            if (s.variant == ISING_VARIANT_MSC) {
+                const long long words = (long long)j.rows * j.nw;
+                for (long long b = 0; b < words; b += 4096)
+                    by_class[kc].push_back(BatchItem{li, 0, b, std::min(words, b + 4096)});
+            } else {
+                const int v = int8_chunk_width(j.lh);
+                L.cpr = j.lh / v;
+                int bx = 1;
+                while (bx < L.cpr && bx < 128) bx <<= 1;
+                L.bx_log2 = __builtin_ctz((unsigned)bx);
+                kc.v = v;
+                kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
+                long long rpi = 16384 / j.lh;
+                if (rpi < 1) rpi = 1;
+                for (long long b = 0; b < j.rows; b += rpi)
+                    by_class[kc].push_back(BatchItem{li, 0, b, std::min<long long>(j.rows, b + rpi)});
+            }
+            lats.push_back(L);
+        }
+        std::vector<BatchItem> items;
+        classes_.clear();
+        for (auto& kv : by_class) {
+            classes_.emplace_back(kv.first, std::make_pair((int)items.size(), (int)kv.second.size()));
+            items.insert(items.end(), kv.second.begin(), kv.second.end());
+        }
+        int rc = upload(lats.data(), lats.size() * sizeof(BatchLattice), (void**)&d_lats_, &lats_cap_);
+        if (rc == ISING_OK)
+            rc = upload(items.data(), items.size() * sizeof(BatchItem), (void**)&d_items_, &items_cap_);
+        dirty_ = false;
+        return rc;
+    }
+
+    int upload(const void* src, size_t bytes, void** dst, size_t* cap)
+    {
+        if (bytes == 0) return ISING_OK;
+        if (bytes > *cap) {
+            if (*dst) cudaFreeAsync(*dst, stream_);
+            size_t nc = std::max(bytes, *cap * 2);
+            cudaError_t e = cudaMallocAsync(dst, nc, stream_);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync (work list)");
+            *cap = nc;
+        }
+        // pageable source: staged by the driver before the call returns
+        cudaError_t e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "work list upload");
+        return ISING_OK;
+    }
+
+    int grid_for(const void* fn, int n_items)
+    {
+        int& per_sm = occupancy_[fn];
+        if (per_sm < 1 &&
+            (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess ||
+             per_sm < 1)) {
+            cudaGetLastError();
+            per_sm = 2;
+        }
+        const int g = sms_ * per_sm;
+        return n_items < g ? n_items : g;
+    }
+
+    template <int V, int NDIM>
+    cudaError_t launch_int8_rule(int rule, const BatchItem* it, int n)
+    {
+        switch (rule) {
+#define ISING_BATCH_CASE(R)                                                                   \
+    case R: {                                                                                 \
+        auto fn = batch_int8_kernel<V, NDIM, R>;                                               \
+        fn<<<grid_for((const void*)fn, n), 256, 0, stream_>>>(d_lats_, it, n, epoch_);        \
+        break;                                                                                \
+    }
+            ISING_BATCH_CASE(kMetroFast)
+            ISING_BATCH_CASE(kHeatFast)
+            ISING_BATCH_CASE(kMetroGeneric)
+            ISING_BATCH_CASE(kHeatGeneric)
+#undef ISING_BATCH_CASE
+        default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_class(const KernelClass& kc, int off, int n)
+    {
+        const BatchItem* it = d_items_ + off;
+        if (kc.variant == ISING_VARIANT_MSC) {
+            auto fn = batch_msc_kernel;
+            fn<<<grid_for((const void*)fn, n), kBatchWarps * 32, 0, stream_>>>(d_lats_, it, n,
+                                                                               epoch_);
+            return cudaGetLastError();
+        }
+        if (kc.ndim == 3) {
+            if (kc.v == 16) return launch_int8_rule<16, 3>(kc.rule, it, n);
+            if (kc.v == 8) return launch_int8_rule<8, 3>(kc.rule, it, n);
+            return launch_int8_rule<4, 3>(kc.rule, it, n);
+        }
+        if (kc.v == 16) return launch_int8_rule<16, 2>(kc.rule, it, n);
+        if (kc.v == 8) return launch_int8_rule<8, 2>(kc.rule, it, n);
+        return launch_int8_rule<4, 2>(kc.rule, it, n);
+    }
+
+    int retire()
+    {
+        for (auto it = active_.begin(); it != active_.end();) {
+            Job& j = *jobs_[*it];
+            if ((epoch_ - j.join_epoch) / 2 >= j.spec.n_sweeps) {
+                int rc = finish_job(j);
+                if (rc != ISING_OK) return rc;
+                it = active_.erase(it);
+                dirty_ = true;
+            } else {
+                ++it;
+            }
+        }
+        return ISING_OK;
+    }
+
+    // Enqueues the result copies after the job's last half-sweep and frees its lattice.
+    int finish_job(Job& j)
+    {
+        cudaError_t e = cudaSuccess;
+        if (j.series_pairs) {
+            const size_t sb = j.series_pairs * 2 * sizeof(long long);
+            e = cudaMallocHost((void**)&j.h_series, sb);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(j.h_series, j.d_series, sb, cudaMemcpyDeviceToHost, stream_);
+        }
+        if (e == cudaSuccess && j.spec.keep_lattice) {
+            const size_t full = (size_t)j.rows * 2 * j.lh;
+            int8_t* stage = nullptr;
+            e = cudaMallocHost((void**)&j.h_lattice, full);
+            if (e == cudaSuccess) e = cudaMallocAsync((void**)&stage, full, stream_);
+            if (e == cudaSuccess) {
+                if (j.spec.variant == ISING_VARIANT_MSC)
+                    e = launch_msc_unpack((const u64*)j.c[0], (const u64*)j.c[1], stage, j.rows, 0,
+                                          j.nw, sms_ * 8, stream_);
+                else
+                    e = launch_int8_merge((const int8_t*)j.c[0], (const int8_t*)j.c[1], stage,
+                                          j.rows, 0, j.lh, j.ly, sms_ * 8, stream_);
+            }
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(j.h_lattice, stage, full, cudaMemcpyDeviceToHost, stream_);
+            if (stage) cudaFreeAsync(stage, stream_);
+        }
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j.done_event, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(j.done_event, stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "job results");
+        for (int c = 0; c < 2; ++c) {
+            cudaFreeAsync(j.c[c], stream_);
+            j.c[c] = nullptr;
+        }
+        if (j.d_series) {
+            cudaFreeAsync(j.d_series, stream_);
+            j.d_series = nullptr;
+        }
+        used_ -= (int64_t)j.device_bytes;
+        j.state = ISING_JOB_FINISHING;
+        finishing_.push_back(j.id);
+        return ISING_OK;
+    }
+
+    // Keeps the host at most kMaxAhead sweeps ahead of the device.
+    int throttle()
+    {
+        static const size_t kMaxAhead = 64;
+        cudaEvent_t ev = nullptr;
+        if (!free_events_.empty()) {
+            ev = free_events_.back();
+            free_events_.pop_back();
+        } else {
+            cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+            epoch_events_.push_back(ev);
+        }
+        cudaEventRecord(ev, stream_);
+        inflight_.push_back(ev);
+        while (inflight_.size() > kMaxAhead) {
+            cudaError_t e = cudaEventSynchronize(inflight_.front());
+            if (e != cudaSuccess) return cuda_fail(e, "throttle");
+            free_events_.push_back(inflight_.front());
+            inflight_.pop_front();
+        }
+        return ISING_OK;
+    }
+
+    void free_job(Job& j, bool shutdown)
+    {
+        if (j.done_event) cudaEventDestroy(j.done_event);
+        j.done_event = nullptr;
+        for (int c = 0; c < 2; ++c)
+            if (j.c[c]) (shutdown ? cudaFree(j.c[c]) : cudaFreeAsync(j.c[c], stream_));
+        if (j.d_series) (shutdown ? cudaFree(j.d_series) : cudaFreeAsync(j.d_series, stream_));
+        if (j.h_series) cudaFreeHost(j.h_series);
+        if (j.h_lattice) cudaFreeHost(j.h_lattice);
+        j.c[0] = j.c[1] = nullptr;
+        j.d_series = nullptr;
+        j.h_series = nullptr;
+        j.h_lattice = nullptr;
+    }
+
+    int device_;
+    int64_t budget_;
+    int64_t used_ = 0;
+    int sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    long long epoch_ = 0;
+    int64_t last_id_ = 0;
+    std::map<int64_t, std::unique_ptr<Job>> jobs_;
+    std::deque<int64_t> pending_;
+    std::vector<int64_t> active_;
+    std::vector<int64_t> finishing_;
+    bool dirty_ = false;
+    BatchLattice* d_lats_ = nullptr;
+    BatchItem* d_items_ = nullptr;
+    size_t lats_cap_ = 0, items_cap_ = 0;
+    std::vector<std::pair<KernelClass, std::pair<int, int>>> classes_;
+    std::vector<cudaEvent_t> epoch_events_, free_events_;
+    std::map<const void*, int> occupancy_;
+    std::deque<cudaEvent_t> inflight_;
+};
+
+}  // namespace ising
+
+using namespace ising;
+
+// ------------------------------------------------------------------------------- batch API ---
+struct ising_batch {
+    std::unique_ptr<Engine> eng;
+};
+
+extern "C" {
+
+int ising_batch_create(int device, int64_t memory_budget, ising_batch** out)
+{
+    if (!out) return fail(ISING_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (memory_budget <= 0) return fail(ISING_ERR_INVALID, "memory budget must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(ISING_ERR_INVALID, "device %d not available", device);
+    }
+    auto b = new ising_batch();
+    b->eng.reset(new Engine(device, memory_budget));
+    int rc = b->eng->init();
+    if (rc != ISING_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return ISING_OK;
+}
+
+int ising_batch_add(ising_batch* b, const ising_job* job, int64_t* id)
+{
+    if (!b || !job || !id) return fail(ISING_ERR_INVALID, "null argument");
+    return b->eng->submit(*job, id);
+}
+
+int ising_batch_run(ising_batch* b, int64_t max_epochs, int64_t* epochs_run)
+{
+    if (!b) return fail(ISING_ERR_INVALID, "null batch");
+    int64_t n = 0;
+    while (b->eng->has_work() && (max_epochs <= 0 || n < max_epochs)) {
+        const size_t before = b->eng->active_count() + b->eng->pending_count();
+        int rc = b->eng->step();
+        if (rc != ISING_OK) return rc;
+        ++n;
+        if (b->eng->active_count() == 0 && b->eng->pending_count() > 0 &&
+            b->eng->pending_count() == before)
+            return fail(ISING_ERR_NOMEM, "pending jobs do not fit the memory budget");
+    }
+    if (epochs_run) *epochs_run = n;
+    return b->eng->wait_finishing();
+}
+
+int ising_batch_status(ising_batch* b, int64_t id, int* state, int64_t* sweeps_done)
+{
+    if (!b || !state) return fail(ISING_ERR_INVALID, "null argument");
+    b->eng->poll();
+    Job* j = b->eng->find(id);
+    if (!j) return fail(ISING_ERR_INVALID, "unknown job %lld", (long long)id);
+    *state = j->state;
+    if (sweeps_done) {
+        long long s = 0;
+        if (j->state == ISING_JOB_DONE || j->state == ISING_JOB_FINISHING) s = j->spec.n_sweeps;
+        else if (j->state == ISING_JOB_ACTIVE) s = (b->eng->epoch() - j->join_epoch) / 2;
+        *sweeps_done = s;
+    }
+    return ISING_OK;
+}
+
+int ising_batch_result(ising_batch* b, int64_t id, int64_t* series_out, int8_t* lattice_out)
+{
+    if (!b) return fail(ISING_ERR_INVALID, "null batch");
+    b->eng->poll();
+    return b->eng->result(id, series_out, lattice_out, nullptr);
+}
+
+int ising_batch_release(ising_batch* b, int64_t id)
+{
+    if (!b) return fail(ISING_ERR_INVALID, "null batch");
+    return b->eng->release(id);
+}
+
+int ising_batch_destroy(ising_batch* b)
+{
+    delete b;
+    return ISING_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------- serving API ---
+struct ising_server {
+    std::unique_ptr<Engine> eng;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false;
+    int error = ISING_OK;
+    std::string error_msg;
+};
+
+static void server_loop(ising_server* s)
+{
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        s->cv_work.wait(lk, [s] { return s->stop || s->eng->busy(); });
+        if (s->stop && !s->eng->busy()) break;
+        if (s->eng->has_work()) {
+            // one sweep (two half-sweeps) per turn, then let submitters in
+            for (int k = 0; k < 2 && s->error == ISING_OK; ++k) {
+                const int rc = s->eng->step();
+                if (rc != ISING_OK) {
+                    s->error = rc;
+                    s->error_msg = g_last_error;
+                }
+            }
+        } else {
+            lk.unlock();
+            cudaStreamSynchronize(s->eng->stream());
+            lk.lock();
+        }
+        if (s->eng->poll() > 0) s->cv_done.notify_all();
+        if (s->error != ISING_OK) {
+            s->cv_done.notify_all();
+            break;
+        }
+        // brief release so submitters and waiters can take the lock
+        lk.unlock();
+        std::this_thread::yield();
+        lk.lock();
+    }
+}
+
+extern "C" {
+
+int ising_server_create(int device, int64_t memory_budget, ising_server** out)
+{
+    if (!out) return fail(ISING_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    if (memory_budget <= 0) return fail(ISING_ERR_INVALID, "memory budget must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(ISING_ERR_INVALID, "device %d not available", device);
+    }
+    auto s = new ising_server();
+    s->eng.reset(new Engine(device, memory_budget));
+    int rc = s->eng->init();
+    if (rc != ISING_OK) {
+        delete s;
+        return rc;
+    }
+    s->worker = std::thread([s, device] {
+        cudaSetDevice(device);
+        server_loop(s);
+    });
+    *out = s;
+    return ISING_OK;
+}
+
+int ising_server_submit(ising_server* s, const ising_job* job, int64_t* id)
+{
+    if (!s || !job || !id) return fail(ISING_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->error != ISING_OK) return fail(s->error, "server stopped: %s", s->error_msg.c_str());
+    int rc = s->eng->submit(*job, id);
+    if (rc == ISING_OK) s->cv_work.notify_one();
+    return rc;
+}
+
+int ising_server_wait(ising_server* s, int64_t id, double timeout_s, int* state)
+{
+    if (!s || !state) return fail(ISING_ERR_INVALID, "null argument");
+    std::unique_lock<std::mutex> lk(s->mu);
+    Job* j = s->eng->find(id);
+    if (!j) return fail(ISING_ERR_INVALID, "unknown job %lld", (long long)id);
+    auto done = [&] { return s->error != ISING_OK || s->eng->find(id)->state == ISING_JOB_DONE; };
+    if (timeout_s < 0) s->cv_done.wait(lk, done);
+    else s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
+    *state = s->eng->find(id)->state;
+    if (s->error != ISING_OK) return fail(s->error, "server stopped: %s", s->error_msg.c_str());
+    return ISING_OK;
+}
+
+int ising_server_result(ising_server* s, int64_t id, int64_t* series_out, int8_t* lattice_out,
+                        double* latency_s)
+{
+    if (!s) return fail(ISING_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->eng->result(id, series_out, lattice_out, latency_s);
+}
+
+int ising_server_release(ising_server* s, int64_t id)
+{
+    if (!s) return fail(ISING_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->eng->release(id);
+}
+
+int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int64_t* used_bytes,
+                        int64_t* epoch)
+{
+    if (!s) return fail(ISING_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (pending) *pending = (int64_t)s->eng->pending_count();
+    if (active) *active = (int64_t)s->eng->active_count();
+    if (used_bytes) *used_bytes = s->eng->used_bytes();
+    if (epoch) *epoch = s->eng->epoch();
+    return ISING_OK;
+}
+
+int ising_server_destroy(ising_server* s)
+{
+    if (!s) return ISING_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    delete s;
+    return ISING_OK;
+}
+
+}  // extern "C"

@@ -316,6 +316,16 @@ int ising_fill_cold(ising_sim* h)
     return ISING_OK;
 }
 
+int ising_fill_philox(ising_sim* h, uint64_t start_seed)
+{
+    CHECK_HANDLE(h);
+    TRY_CUDA(cudaSetDevice(h->device));
+    TRY_CUDA(launch_philox_start(h->c[0], h->c[1], h->rows * (long long)h->lh,
+                                 h->variant == ISING_VARIANT_MSC, (u32)start_seed,
+                                 (u32)(start_seed >> 32), h->max_blocks, h->stream));
+    return ISING_OK;
+}
+
 int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
                 int64_t* series_out)
 {

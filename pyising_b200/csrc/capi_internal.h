@@ -61,6 +61,8 @@ cudaError_t launch_msc_pack(const int8_t* full, u64* w0, u64* w1, int rows, int 
                             int max_blocks, cudaStream_t st);
 cudaError_t launch_msc_unpack(const u64* w0, const u64* w1, int8_t* full, int rows, int row0,
                               int nw, int max_blocks, cudaStream_t st);
+cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
+                                int max_blocks, cudaStream_t st);
 cudaError_t launch_philox_probe(u32* out, int blocks, int threads, int calls, u32 k0, u32 k1,
                                 cudaStream_t st);
 cudaError_t launch_philox_range(u32* out, long long n, u32 q0, u32 c1, u32 c2, u32 c3, u32 k0,

@@ -1,146 +1,12 @@
-// int8 compressed-checkerboard half-sweep (2D/3D, Metropolis/heat bath) with the fused
-// integer (M, E) reduction.
-//
-// Same results as pyising's NumpyCheckerboard._half_sweep (src/pyising/backends/
-// numpy_backend.py:26-44) and the CUDA C int8_half kernel (src/pyising/backends/cuda/
-// ising.cu:25-87): site n = row*Lh + j of colour c draws word n%4 of
-// Philox((n/4, t, c, 0), seed) (src/pyising/philox.py:54-64).
-//
-// Work split: a thread owns V consecutive colour sites of one row (V = 16: one 128-bit load
-// per array, four Philox blocks).  Spins stay packed in 32-bit words and the neighbour
-// counting is byte-parallel (SWAR): with +1 = 0x01 and -1 = 0xFF, bit 1 of each byte is the
-// "down" flag, so (a ^ b) & 0x02020202 marks anti-aligned pairs of four sites at once.
-//
-// Decision without table lookups.  Metropolis flips iff X <= 0 or u < table[(X + 2d)/2] with
-// X = s*h = 2d - 2A (A = anti-aligned neighbours).  Let T(a) = table[2d - a] for a < d; threshold
-// tables built by threshold_table() make T non-decreasing in a, so with
-// L = #{a < d : u < T(a)} the rule is exactly "flip iff A + L >= d".  Heat bath sets +1 iff
-// u < table[U] (U = up neighbours = 2d - D); with the table non-decreasing and
-// L = #{k <= 2d : u < table[k]} this is "up iff L > D".  Both comparisons run byte-parallel.
-// Tables that are not monotone use the generic per-site lookup rules.
-#include "common.cuh"
+// int8 compressed-checkerboard half-sweep kernel (2D/3D, Metropolis/heat bath) with the fused
+// integer (M, E) reduction; the per-chunk update is int8_chunk in int8_core.cuh.
+#include "int8_core.cuh"
 
 namespace ising {
-
-template <int W>
-struct Words {
-    u32 v[W];
-};
-
-template <int W>
-__device__ __forceinline__ Words<W> load_words(const int8_t* p)
-{
-    Words<W> r;
-    if constexpr (W == 4) {
-        const uint4 q = *reinterpret_cast<const uint4*>(p);
-        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
-    } else if constexpr (W == 2) {
-        const uint2 q = *reinterpret_cast<const uint2*>(p);
-        r.v[0] = q.x; r.v[1] = q.y;
-    } else {
-        r.v[0] = *reinterpret_cast<const u32*>(p);
-    }
-    return r;
-}
-
-template <int W>
-__device__ __forceinline__ Words<W> load_words_ro(const int8_t* p)
-{
-    Words<W> r;
-    if constexpr (W == 4) {
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(p));
-        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
-    } else if constexpr (W == 2) {
-        const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
-        r.v[0] = q.x; r.v[1] = q.y;
-    } else {
-        r.v[0] = __ldg(reinterpret_cast<const unsigned int*>(p));
-    }
-    return r;
-}
-
-template <int W>
-__device__ __forceinline__ void store_words(int8_t* p, const Words<W>& r)
-{
-    if constexpr (W == 4) {
-        *reinterpret_cast<uint4*>(p) = make_uint4(r.v[0], r.v[1], r.v[2], r.v[3]);
-    } else if constexpr (W == 2) {
-        *reinterpret_cast<uint2*>(p) = make_uint2(r.v[0], r.v[1]);
-    } else {
-        *reinterpret_cast<u32*>(p) = r.v[0];
-    }
-}
-
-__device__ __forceinline__ u32 table_at(const Int8Half& p, int i)
-{
-    // Constant indices only, so the table stays in the kernel parameter bank.
-    u32 v = p.table[0];
-    v = i == 1 ? p.table[1] : v;
-    v = i == 2 ? p.table[2] : v;
-    v = i == 3 ? p.table[3] : v;
-    v = i == 4 ? p.table[4] : v;
-    v = i == 5 ? p.table[5] : v;
-    v = i == 6 ? p.table[6] : v;
-    return v;
-}
-
-// New spins of the four sites in word `s` given their anti-aligned (Metropolis) or down
-// (heat bath) neighbour counts `cnt` (one byte per site) and their four uniforms.
-template <int NDIM, int RULE>
-__device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const u32x4& r)
-{
-    constexpr int d = NDIM;
-    if constexpr (RULE == kObserve) {
-        return s;
-    } else if constexpr (RULE == kMetroFast) {
-        u32 l[4] = {0, 0, 0, 0};
-        const u32 uu[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-        for (int a = 0; a < d; ++a) {
-            const u32 thr = p.table[2 * d - a];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) l[i] += uu[i] < thr ? 1u : 0u;
-        }
-        const u32 lw = l[0] | (l[1] << 8) | (l[2] << 16) | (l[3] << 24);
-        const u32 m7 = (cnt + lw + (u32)(0x80 - d) * 0x01010101u) & kBit7;
-        return s ^ flip_mask_from_bit7(m7);
-    } else if constexpr (RULE == kHeatFast) {
-        u32 l[4] = {0, 0, 0, 0};
-        const u32 uu[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-        for (int k = 0; k <= 2 * d; ++k) {
-            const u32 thr = p.table[k];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) l[i] += uu[i] < thr ? 1u : 0u;
-        }
-        const u32 lw = l[0] | (l[1] << 8) | (l[2] << 16) | (l[3] << 24);
-        const u32 m7 = (lw + 0x7F7F7F7Fu - cnt) & kBit7;  // up iff L > D
-        return 0xFFFFFFFFu ^ flip_mask_from_bit7(m7);
-    } else {
-        const u32 uu[4] = {r.x, r.y, r.z, r.w};
-        u32 out = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int c = (int)((cnt >> (8 * i)) & 0xFFu);
-            const u32 sb = (s >> (8 * i)) & 0xFFu;
-            u32 nb;
-            if constexpr (RULE == kMetroGeneric) {
-                const bool flip = c >= d || uu[i] < table_at(p, 2 * d - c);
-                nb = flip ? (sb ^ 0xFEu) : sb;
-            } else {
-                nb = uu[i] < table_at(p, 2 * d - c) ? 0x01u : 0xFFu;
-            }
-            out |= nb << (8 * i);
-        }
-        return out;
-    }
-}
 
 template <int V, int NDIM, int RULE>
 __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
 {
-    constexpr int W = V / 4;
-    constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
     const int jc = blockIdx.x * blockDim.x + threadIdx.x;
     long long m_acc = 0, e_acc = 0;
     if (jc < p.cpr) {
@@ -168,82 +34,7 @@ __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
             } else {
                 y = (int)row;
             }
-            const int par = (y + z + (int)p.color) & 1;
-            const long long rb = row * p.lh;
-            const int8_t* orow = p.other + rb;
-
-            const Words<W> s = load_words<W>(p.own + rb + j0);
-            const Words<W> c = load_words_ro<W>(orow + j0);
-            const int yu = z * p.ly + (y + 1 == p.ly ? 0 : y + 1);
-            const int yd = z * p.ly + (y == 0 ? p.ly - 1 : y - 1);
-            const Words<W> nu = load_words_ro<W>(p.other + (long long)yu * p.lh + j0);
-            const Words<W> nd = load_words_ro<W>(p.other + (long long)yd * p.lh + j0);
-            Words<W> zu, zd;
-            if constexpr (NDIM == 3) {
-                const int pu = (z + 1 == p.lz ? 0 : z + 1) * p.ly + y;
-                const int pd = (z == 0 ? p.lz - 1 : z - 1) * p.ly + y;
-                zu = load_words_ro<W>(p.other + (long long)pu * p.lh + j0);
-                zd = load_words_ro<W>(p.other + (long long)pd * p.lh + j0);
-            }
-            // horizontal neighbour byte outside this chunk (periodic in x)
-            const int je = par ? (j0 + V == p.lh ? 0 : j0 + V) : (j0 == 0 ? p.lh - 1 : j0 - 1);
-            const u32 edge = (u32)(uint8_t)__ldg(orow + je);
-
-            Words<W> hz;
-#pragma unroll
-            for (int k = 0; k < W; ++k) {
-                if (par) {
-                    const u32 nx = (k + 1 < W) ? c.v[(k + 1) % W] : edge;
-                    hz.v[k] = __funnelshift_r(c.v[k], nx, 8);
-                } else {
-                    const u32 pv = (k > 0) ? c.v[(k + W - 1) % W] : (edge << 24);
-                    hz.v[k] = __funnelshift_l(pv, c.v[k], 8);
-                }
-            }
-
-            Words<W> ns;
-            const u32 q0 = (u32)((unsigned long long)(rb + j0) >> 2);
-#pragma unroll
-            for (int k = 0; k < W; ++k) {
-                u32 cnt;
-                if constexpr (kHeat) {
-                    u32 acc = (c.v[k] & kBit1) + (hz.v[k] & kBit1) + (nu.v[k] & kBit1) +
-                              (nd.v[k] & kBit1);
-                    if constexpr (NDIM == 3) acc += (zu.v[k] & kBit1) + (zd.v[k] & kBit1);
-                    cnt = acc >> 1;  // down neighbours per site
-                } else {
-                    const u32 sv = s.v[k];
-                    u32 acc = ((c.v[k] ^ sv) & kBit1) + ((hz.v[k] ^ sv) & kBit1) +
-                              ((nu.v[k] ^ sv) & kBit1) + ((nd.v[k] ^ sv) & kBit1);
-                    if constexpr (NDIM == 3)
-                        acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
-                    cnt = acc >> 1;  // anti-aligned neighbours per site
-                }
-                if constexpr (RULE == kObserve) {
-                    ns.v[k] = s.v[k];
-                } else {
-                    const u32x4 r = philox4x32_10(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
-                    ns.v[k] = decide4<NDIM, RULE>(p, s.v[k], cnt, r);
-                }
-            }
-            if constexpr (RULE != kObserve) store_words<W>(p.own + rb + j0, ns);
-
-            if (p.meas) {
-                // Bonds of this colour's sites: s*h = 2d - 2A per site; E = -sum s*h.
-                int anti = 0, down = 0;
-#pragma unroll
-                for (int k = 0; k < W; ++k) {
-                    const u32 sv = ns.v[k];
-                    u32 acc = ((c.v[k] ^ sv) & kBit1) + ((hz.v[k] ^ sv) & kBit1) +
-                              ((nu.v[k] ^ sv) & kBit1) + ((nd.v[k] ^ sv) & kBit1);
-                    if constexpr (NDIM == 3)
-                        acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
-                    anti += byte_sum(acc >> 1);
-                    down += __popc(sv & kBit1) + __popc(c.v[k] & kBit1);
-                }
-                m_acc += 2 * V - 2 * down;          // this colour's V sites + the other's V
-                e_acc += 2 * anti - 2 * NDIM * V;   // -(2d V - 2 anti)
-            }
+            int8_chunk<V, NDIM, RULE>(p, row, y, z, j0, m_acc, e_acc);
         }
     }
     if (p.meas) block_accumulate2(m_acc, e_acc, p.meas);

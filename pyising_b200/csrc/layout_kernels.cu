@@ -104,6 +104,51 @@ __global__ void msc_unpack_kernel(const u64* __restrict__ w0, const u64* __restr
     }
 }
 
+// Device seeded start (not in the reference, whose hot start is NumPy's PCG64): compressed site
+// n of colour c is +1 iff bit n % 32 of word (n / 32) % 4 of Philox((n / 128, 0, c, 0xFFFFFFFF),
+// seed) is set.  Counter word 3 = 0xFFFFFFFF is never used by a sweep, and int8 and packed
+// layouts get the same spins.  One thread per colour and 128-site group; `sites` = sites per
+// colour (rows * Lx/2).
+__global__ void philox_start_kernel(void* c0, void* c1, long long sites, int packed, u32 k0,
+                                    u32 k1)
+{
+    const long long groups = (sites + 127) / 128;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < 2 * groups;
+         i += (long long)gridDim.x * blockDim.x) {
+        const u32 color = (u32)(i / groups);
+        const long long g = i - (long long)color * groups;
+        const u32x4 r = philox4x32_10((u32)g, 0u, color, 0xFFFFFFFFu, k0, k1);
+        const u32 rw[4] = {r.x, r.y, r.z, r.w};
+        void* dst = color ? c1 : c0;
+        if (packed) {  // words 2g and 2g+1 (sites is a multiple of 128 for the packed layout)
+            u64* w = static_cast<u64*>(dst) + 2 * g;
+            w[0] = (u64)r.x | ((u64)r.y << 32);
+            w[1] = (u64)r.z | ((u64)r.w << 32);
+        } else {
+            int8_t* b = static_cast<int8_t*>(dst) + 128 * g;
+            const long long left = sites - 128 * g;
+            for (int m = 0; m < 32; ++m) {  // 4 sites per m: bits 4m'..4m'+3 of one word
+                if (4 * m >= left) break;
+                const u32 nib = (rw[m >> 3] >> (4 * (m & 7))) & 0xFu;
+                const u32 ones = (nib * 0x00204081u) & 0x01010101u;  // bit i -> byte i
+                const u32 v = 0xFFFFFFFFu ^ (ones * 0xFEu);           // 1 -> +1, 0 -> -1
+                reinterpret_cast<u32*>(b)[m] = v;
+            }
+        }
+    }
+}
+
+cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
+                                int max_blocks, cudaStream_t st)
+{
+    const long long work = 2 * ((sites + 127) / 128);
+    long long g = (work + 255) / 256;
+    if (g > max_blocks) g = max_blocks;
+    if (g < 1) g = 1;
+    philox_start_kernel<<<(unsigned)g, 256, 0, st>>>(c0, c1, sites, packed, k0, k1);
+    return cudaGetLastError();
+}
+
 // Throughput probe: `calls` Philox blocks per thread, outputs xor-folded so nothing is dead.
 __global__ void philox_probe_kernel(u32* __restrict__ out, int calls, u32 k0, u32 k1)
 {

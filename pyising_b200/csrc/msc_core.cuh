@@ -1,0 +1,279 @@
+// Device code of the multi-spin-coded (64 spins per uint64) 2D Metropolis half-sweep with the
+// lazy bitwise uniform comparison, shared by the single-lattice and the batched kernels.
+//
+// Same results as pyising's NumpyMultiSpin (src/pyising/backends/numpy_backend.py:54-124) and
+// the CUDA C msc_half kernel (src/pyising/backends/cuda/ising.cu:92-150): word w at bit level
+// k uses call k/2 of Philox((w, t, c, 1 + k/2), seed); even levels take r0 | r1 << 32, odd
+// levels r2 | r3 << 32 (src/pyising/philox.py:67-78).  Level k decides the lanes whose
+// uniform's bit 31-k differs from the threshold's: u < thr exactly when, at the first
+// differing bit, u has 0 and the threshold has 1.
+#pragma once
+
+#include "common.cuh"
+
+#ifndef ISING_MSC_INTAKE_CALLS
+#define ISING_MSC_INTAKE_CALLS 4
+#endif
+
+namespace ising {
+
+// Bit-sliced anti-aligned count of the four neighbours: a0 = none, a1 = exactly one,
+// a2 = two or more (numpy_backend.py:63-69).
+struct Slices {
+    u64 a0, a1, a2;
+};
+
+__device__ __forceinline__ Slices slice4(u64 o, u64 n1, u64 n2, u64 n3, u64 n4)
+{
+    const u64 x1 = o ^ n1, x2 = o ^ n2, x3 = o ^ n3, x4 = o ^ n4;
+    const u64 any = x1 | x2 | x3 | x4;
+    const u64 s1 = x1 ^ x2, c1 = x1 & x2, s2 = x3 ^ x4, c2 = x3 & x4;
+    Slices s;
+    s.a2 = c1 | c2 | (s1 & s2);
+    s.a1 = any & ~s.a2;
+    s.a0 = ~any;
+    return s;
+}
+
+__device__ __forceinline__ void lazy_level(u64 r, int bit, u32 thr4, u32 thr8, const Slices& s,
+                                           u64& acc, u64& und)
+{
+    const u64 t4 = ((thr4 >> bit) & 1u) ? ~0ull : 0ull;
+    const u64 t8 = ((thr8 >> bit) & 1u) ? ~0ull : 0ull;
+    const u64 tm = (s.a1 & t4) | (s.a0 & t8);
+    acc |= und & ~r & tm;
+    und &= ~(r ^ tm);
+}
+
+// Flip mask of one word drawing Philox blocks until every lane is decided; `calls` returns
+// the blocks drawn.
+__device__ __forceinline__ u64 msc_flip(const Slices& s, u32 w, u32 t, u32 color, u32 k0,
+                                        u32 k1, u32 thr4, u32 thr8, int& calls)
+{
+    u64 acc = 0, und = s.a0 | s.a1;
+    int lp = 0;
+    for (; lp < 16 && und; ++lp) {
+        const u32x4 r = philox4x32_10(w, t, color, 1u + (u32)lp, k0, k1);
+        lazy_level((u64)r.x | ((u64)r.y << 32), 31 - 2 * lp, thr4, thr8, s, acc, und);
+        lazy_level((u64)r.z | ((u64)r.w << 32), 30 - 2 * lp, thr4, thr8, s, acc, und);
+    }
+    calls = lp;
+    return s.a2 | acc;
+}
+
+// One word (row y, word x): update when UPDATE, then the (M, E) contribution of its 64 sites'
+// bonds when p.meas (every bond has exactly one colour-1 end; the other colour's same-index
+// word is counted once for M), and the call statistics when p.stats.
+template <bool UPDATE>
+__device__ __forceinline__ void msc_word(const MscHalf& p, int y, int x, long long& m_acc,
+                                         long long& e_acc, long long& calls_acc,
+                                         long long& wmax_acc)
+{
+    const int nw = p.nw;
+    const long long rb = (long long)y * nw;
+    const u64* orow = p.other + rb;
+    const u64 o = p.own[rb + x];
+    const u64 c = __ldg(orow + x);
+    u64 hz;
+    if ((y + (int)p.color) & 1) hz = (c >> 1) | (__ldg(orow + (x + 1 == nw ? 0 : x + 1)) << 63);
+    else hz = (c << 1) | (__ldg(orow + (x == 0 ? nw - 1 : x - 1)) >> 63);
+    const u64 up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
+    const u64 dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
+    u64 ns = o;
+    if constexpr (UPDATE) {
+        const Slices s = slice4(o, c, hz, up, dn);
+        int calls = 0;
+        ns = o ^ msc_flip(s, (u32)(rb + x), p.t, p.color, p.k0, p.k1, p.thr4, p.thr8, calls);
+        p.own[rb + x] = ns;
+        if (p.stats) {
+            calls_acc += calls;
+            wmax_acc += __reduce_max_sync(__activemask(), calls);
+        }
+    }
+    if (p.meas) {
+        const int anti =
+            __popcll(ns ^ c) + __popcll(ns ^ hz) + __popcll(ns ^ up) + __popcll(ns ^ dn);
+        m_acc += 2 * (__popcll(ns) + __popcll(c)) - 128;
+        e_acc += 2 * anti - 256;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Work-stack schedule (no measurement): keeps every lane busy with a Philox block.
+//
+// Per word, the lazy comparison needs a data-dependent number of Philox blocks (3.8 on average
+// at T_c, but 6.3 for the slowest word of a warp), so a one-word-per-lane kernel idles most
+// lanes in its last iterations.  Here a warp walks a contiguous range of words:
+//   * intake: the next 32 words of the range (their global loads were issued when the previous
+//     batch was consumed) are bit-sliced and get four Philox blocks each unconditionally (at
+//     T_c half of the words need four or more); decided words are stored, the others pushed on
+//     the warp's 64-entry stack in shared memory;
+//   * while the stack holds 32 or more entries (or the range is done): pop up to 32, draw one
+//     Philox block each at the entry's own level pair, store finished words, push back the rest.
+// The random numbers, bit levels and their order are the reference's; only the schedule
+// differs, so results are identical.  Lanes are handled as two independent 32-bit halves.
+
+constexpr int kQueueCap = 64;
+constexpr int kIntakeCalls = ISING_MSC_INTAKE_CALLS;  // Philox blocks per word before queueing
+
+struct QueueSlots {
+    u32 idx[kQueueCap];
+    u32 lp[kQueueCap];
+    u64 a1[kQueueCap];
+    u64 und[kQueueCap];
+    u64 res[kQueueCap];
+};
+
+// Threshold bit masks of the even and odd level of each level pair: (t4e, t8e, t4o, t8o).
+__device__ __forceinline__ uint4 level_masks(u32 thr4, u32 thr8, u32 lp)
+{
+    const u32 se = 31u - 2u * lp, so = se - 1u;
+    return make_uint4(((thr4 >> se) & 1u) ? ~0u : 0u, ((thr8 >> se) & 1u) ? ~0u : 0u,
+                      ((thr4 >> so) & 1u) ? ~0u : 0u, ((thr8 >> so) & 1u) ? ~0u : 0u);
+}
+
+// One bit level on 32 lanes: tm selects each lane's threshold bit (thr4 for lanes with one
+// anti-aligned neighbour, thr8 for none); an undecided lane is decided when its random bit
+// differs from tm, and accepted (flipped) when that bit is 0 and tm is 1.
+__device__ __forceinline__ void level32(u32 r, u32 t4m, u32 t8m, u32 a1, u32& und, u32& res)
+{
+    const u32 tm = (a1 & t4m) | (~a1 & t8m);
+    res ^= und & ~r & tm;
+    und &= ~(r ^ tm);
+}
+
+__device__ __forceinline__ void call_levels(const u32x4& r, const uint4& m, u32 a1l, u32 a1h,
+                                            u32& undl, u32& undh, u32& resl, u32& resh)
+{
+    level32(r.x, m.x, m.y, a1l, undl, resl);  // even level: r0 | r1 << 32
+    level32(r.y, m.x, m.y, a1h, undh, resh);
+    level32(r.z, m.z, m.w, a1l, undl, resl);  // odd level: r2 | r3 << 32
+    level32(r.w, m.z, m.w, a1h, undh, resh);
+}
+
+// Global words of one intake batch (one per lane), loaded ahead of use.
+struct IntakeLoads {
+    u64 o, c, side, up, dn;
+};
+
+__device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool valid, int nw,
+                                            int nw_shift, IntakeLoads& L)
+{
+    if (!valid) {
+        L.o = L.c = L.side = L.up = L.dn = 0;
+        return;
+    }
+    int y, x;
+    if (nw_shift >= 0) {
+        y = (int)(w >> nw_shift);
+        x = (int)(w & (nw - 1));
+    } else {
+        y = (int)(w / nw);
+        x = (int)(w - (long long)y * nw);
+    }
+    const u64* orow = p.other + (long long)y * nw;
+    L.o = p.own[w];
+    L.c = __ldg(orow + x);
+    const int xs = ((y + (int)p.color) & 1) ? (x + 1 == nw ? 0 : x + 1) : (x == 0 ? nw - 1 : x - 1);
+    L.side = __ldg(orow + xs);
+    L.up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
+    L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
+}
+
+// The whole warp updates words [begin, end) of the lattice in p.  `lvmask` holds
+// level_masks(p.thr4, p.thr8, lp) for lp = 0..15; `q` is this warp's stack.
+__device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begin, long long end,
+                                                int nw_shift, QueueSlots& q,
+                                                const uint4* lvmask)
+{
+    const int lane = threadIdx.x & 31;
+    const u32 lt = (1u << lane) - 1u;
+    const int nw = p.nw;
+    long long next = begin;
+    int n = 0;
+    IntakeLoads L;
+    long long w = next + lane;
+    bool more = next < end;
+    if (more) intake_load(p, w, w < end, nw, nw_shift, L);
+    while (true) {
+        if (n < 32 && more) {
+            const bool valid = w < end;
+            u32 a1l = 0, a1h = 0, undl = 0, undh = 0, resl = 0, resh = 0;
+            if (valid) {
+                const int yw = (int)(nw_shift >= 0 ? (w >> nw_shift) : (w / nw));
+                const bool par = (yw + (int)p.color) & 1;
+                const u64 hz = par ? ((L.c >> 1) | (L.side << 63)) : ((L.c << 1) | (L.side >> 63));
+                const Slices s = slice4(L.o, L.c, hz, L.up, L.dn);
+                a1l = (u32)s.a1;
+                a1h = (u32)(s.a1 >> 32);
+                undl = ~(u32)s.a2;
+                undh = ~(u32)(s.a2 >> 32);
+                const u64 r0 = L.o ^ s.a2;
+                resl = (u32)r0;
+                resh = (u32)(r0 >> 32);
+            }
+            const long long wc = w;
+            next += 32;
+            more = next < end;
+            w = next + lane;
+            if (more) intake_load(p, w, w < end, nw, nw_shift, L);
+            if (valid) {
+#pragma unroll
+                for (int c3 = 0; c3 < kIntakeCalls; ++c3) {
+                    const u32x4 r = philox4x32_10((u32)wc, p.t, p.color, 1u + (u32)c3, p.k0, p.k1);
+                    call_levels(r, lvmask[c3], a1l, a1h, undl, undh, resl, resh);
+                }
+            }
+            const bool keep = valid && (undl | undh) != 0;
+            if (valid && !keep) p.own[wc] = (u64)resl | ((u64)resh << 32);
+            const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
+            if (keep) {
+                const int pos = n + __popc(km & lt);
+                q.idx[pos] = (u32)wc;
+                q.lp[pos] = (u32)kIntakeCalls;
+                q.a1[pos] = (u64)a1l | ((u64)a1h << 32);
+                q.und[pos] = (u64)undl | ((u64)undh << 32);
+                q.res[pos] = (u64)resl | ((u64)resh << 32);
+            }
+            n += __popc(km);
+            __syncwarp();
+        } else if (n > 0) {
+            const int take = n < 32 ? n : 32;
+            const int base = n - take;
+            const bool act = lane < take;
+            u32 idx = 0, lp = 0;
+            u64 a1 = 0, und = 0, res = 0;
+            if (act) {
+                idx = q.idx[base + lane];
+                lp = q.lp[base + lane];
+                a1 = q.a1[base + lane];
+                und = q.und[base + lane];
+                res = q.res[base + lane];
+            }
+            __syncwarp();
+            u32 undl = (u32)und, undh = (u32)(und >> 32), resl = (u32)res, resh = (u32)(res >> 32);
+            if (act) {
+                const u32x4 r = philox4x32_10(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
+                call_levels(r, lvmask[lp], (u32)a1, (u32)(a1 >> 32), undl, undh, resl, resh);
+                ++lp;
+            }
+            const bool keep = act && (undl | undh) != 0 && lp < 16u;
+            if (act && !keep) p.own[idx] = (u64)resl | ((u64)resh << 32);
+            const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
+            if (keep) {
+                const int pos = base + __popc(km & lt);
+                q.idx[pos] = idx;
+                q.lp[pos] = lp;
+                q.a1[pos] = a1;
+                q.und[pos] = (u64)undl | ((u64)undh << 32);
+                q.res[pos] = (u64)resl | ((u64)resh << 32);
+            }
+            n = base + __popc(km);
+            __syncwarp();
+        } else {
+            break;
+        }
+    }
+}
+
+}  // namespace ising
