@@ -55,7 +55,7 @@ DESCRIPTION = {
                    "with (E, M) every 10 sweeps",
 }
 MEASURE_EVERY = {"int8_3d_256": 10}
-KERNEL = {"msc": "msc_half_kernel", "int8": "int8_half_kernel"}
+KERNEL = {"msc": "msc_half_queue_kernel", "int8": "int8_half_kernel"}
 
 
 # ------------------------------------------------------------------------- helpers -------
@@ -293,6 +293,148 @@ def cpu_baseline(wl: str, budget_s: float = 10.0) -> dict:
                       f"{alg}) on the C oracle, {cores} threads, {dt:.1f} s"}
 
 
+TC_3D = 1.0 / BETA_3D
+
+
+def c4_jobs(sweeps: int = 5000, every: int = 10):
+    """The batched-ensemble config: 96 2D int8 Metropolis lattices, L = 2^k with k uniform in
+    6..12, T uniform in [2.0, 2.6], seed = index, NumPy hot start; draws from default_rng(0)."""
+    from pyising_b200.ensemble import Job
+    from pyising_b200.lattice import random_lattice
+
+    rng = np.random.default_rng(0)
+    ks = rng.integers(6, 13, size=96)
+    Ts = rng.uniform(2.0, 2.6, size=96)
+    return [Job((2 ** int(k), 2 ** int(k)), 1.0 / float(T), sweeps, seed=i, measure_every=every,
+                init=random_lattice((2 ** int(k), 2 ** int(k)), i))
+            for i, (k, T) in enumerate(zip(ks, Ts, strict=True))]
+
+
+def c5_jobs(n_jobs: int, seed: int = 2026):
+    """The served-stream config: Poisson arrivals at 200 jobs/s; 70% 2D (L log-uniform in
+    128..8192, int8 or msc 50/50, Metropolis, T within +-15% of T_c), 30% 3D (L log-uniform in
+    32..256, int8 heat bath, T within +-15% of the 3D T_c); sweeps log-uniform in 100..10000;
+    (M, E) every 10 sweeps; L rounded to the layout multiple; device seeded start (seed = index).
+    Returns (arrival times in s, jobs)."""
+    from pyising_b200.ensemble import Job
+
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, size=n_jobs))
+    jobs = []
+    for i in range(n_jobs):
+        sweeps = int(np.exp(rng.uniform(np.log(100), np.log(10000))))
+        if rng.random() < 0.7:
+            variant = "msc" if rng.random() < 0.5 else "int8"
+            m = 128 if variant == "msc" else 8
+            L = int(np.exp(rng.uniform(np.log(128), np.log(8192))))
+            L = max(m, int(round(L / m)) * m)
+            T = (1.0 / BETA_C_2D) * rng.uniform(0.85, 1.15)
+            jobs.append(Job((L, L), 1.0 / T, sweeps, seed=i, variant=variant, measure_every=10,
+                            init="philox"))
+        else:
+            L = int(np.exp(rng.uniform(np.log(32), np.log(256))))
+            L = max(8, int(round(L / 8)) * 8)
+            T = TC_3D * rng.uniform(0.85, 1.15)
+            jobs.append(Job((L, L, L), 1.0 / T, sweeps, seed=i, algorithm="heatbath",
+                            measure_every=10, init="philox"))
+    return arrivals, jobs
+
+
+def sequential_plain(jobs) -> tuple[float, list]:
+    """The same jobs one at a time through the single-lattice API (upload or device start,
+    sweeps with the fused measurement, series back to the host); returns (seconds, series)."""
+    import torch
+
+    from pyising_b200.backend import B200Int8, B200MultiSpin
+
+    out = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j in jobs:
+        cls = B200MultiSpin if j.variant == "msc" else B200Int8
+        sim = cls(j.shape, j.beta, seed=j.seed, algorithm=j.algorithm, init=j.init)
+        out.append(sim.sweep_measured(j.sweeps, j.measure_every))
+        del sim
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, out
+
+
+def run_batched_ensemble() -> dict:
+    """C4: batched vs one at a time, every lattice's series compared."""
+    import torch
+
+    from pyising_b200.ensemble import Ensemble
+
+    jobs = c4_jobs()
+    flips = sum(j.n_spins * j.sweeps for j in jobs)
+    with Ensemble(memory_budget=120e9) as ens:
+        ids = [ens.add(j) for j in jobs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.run()
+        t_batch = time.perf_counter() - t0
+        batched = [ens.result(i).series for i in ids]
+    t_seq, seq = sequential_plain(jobs)
+    same = all(np.array_equal(a, b) for a, b in zip(batched, seq, strict=True))
+    return {"workload": "96 2D int8 Metropolis lattices, L=2^k k~U{6..12}, T~U[2.0,2.6], "
+                        "seed=index, NumPy hot start, 5000 sweeps, (E,M) every 10; "
+                        "draws from default_rng(0)",
+            "flips": flips, "batched_s": round(t_batch, 3), "sequential_s": round(t_seq, 3),
+            "batched_flips_per_ns": round(flips / t_batch / 1e9, 2),
+            "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
+            "speedup": round(t_seq / t_batch, 3), "bit_identical": bool(same),
+            "timed": "uploads of the start lattices, all sweeps, series back to the host"}
+
+
+def run_served_stream(n_jobs: int) -> dict:
+    """C5 (scaled to n_jobs): Poisson arrivals into the server; vs one at a time."""
+    import threading
+
+    from pyising_b200.ensemble import Server
+
+    arrivals, jobs = c5_jobs(n_jobs)
+    flips = sum(j.n_spins * j.sweeps for j in jobs)
+    submit_t = [0.0] * n_jobs
+    ids = [0] * n_jobs
+    with Server(memory_budget=120e9) as srv:
+        start = time.perf_counter()
+
+        def feeder():
+            for i, job in enumerate(jobs):
+                delay = start + arrivals[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                submit_t[i] = time.perf_counter()
+                ids[i] = srv.submit(job)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        results = []
+        for i in range(n_jobs):
+            srv.wait(ids[i])
+            results.append(srv.result(ids[i]))
+            srv.release(ids[i])
+    lat = np.array([r.latency_s for r in results])
+    end = max(submit_t[i] + lat[i] for i in range(n_jobs))
+    served_s = end - submit_t[0]
+    t_seq, seq = sequential_plain(jobs)
+    same = all(np.array_equal(r.series, s) for r, s in zip(results, seq, strict=True))
+    return {"workload": f"{n_jobs} jobs of the served-stream mix (Poisson 200 jobs/s; 70% 2D "
+                        "L~logU[128,8192] int8|msc, 30% 3D L~logU[32,256] int8 heat bath; "
+                        "T_c +-15%; sweeps~logU[100,10000]; (E,M) every 10; device seeded "
+                        "start), seed 2026",
+            "jobs": n_jobs, "flips": flips, "offered_flips_per_ns": round(
+                flips / (arrivals[-1] * 1e9), 2),
+            "served_s": round(served_s, 3), "served_flips_per_ns": round(flips / served_s / 1e9, 2),
+            "sequential_s": round(t_seq, 3),
+            "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
+            "speedup": round(t_seq / served_s, 3),
+            "latency_p50_s": round(float(np.percentile(lat, 50)), 4),
+            "latency_p99_s": round(float(np.percentile(lat, 99)), 4),
+            "bit_identical": bool(same), "memory_budget_bytes": int(120e9)}
+
+
 def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
     import torch
 
@@ -352,6 +494,10 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
                              "pct_hbm_roofline": round(100 * d["value"] * b / peaks["hbm_gbs"], 2),
                              "description": DESCRIPTION[other]}
         line["other_configs"] = extras
+    if args.batch and world == 1:
+        line["batched_ensemble"] = run_batched_ensemble()
+    if args.serve_jobs > 0 and world == 1:
+        line["served_stream"] = run_served_stream(args.serve_jobs)
     torch.cuda.synchronize()
     return line
 
@@ -404,6 +550,10 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="msc16384")
     ap.add_argument("--no-extras", dest="extras", action="store_false")
+    ap.add_argument("--no-batch", dest="batch", action="store_false",
+                    help="skip the 96-lattice batched ensemble")
+    ap.add_argument("--serve-jobs", type=int, default=300,
+                    help="jobs of the served stream (0 = skip)")
     ap.add_argument("--cpu-budget", type=float, default=10.0,
                     help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--ref-step-s", type=float, default=2.0,
