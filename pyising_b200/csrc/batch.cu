@@ -55,10 +55,13 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
                                                          const BatchItem* __restrict__ items,
                                                          int n_items, long long epoch)
 {
+    __shared__ u32 stab[8];  // this item's acceptance table for the per-site lookup rules
     const u32 color = (u32)(epoch & 1);
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const BatchLattice& L = lats[item.lat];
+        if (threadIdx.x < 7) stab[threadIdx.x] = L.table[threadIdx.x];
+        __syncthreads();
         const long long s = (epoch - L.join_epoch) >> 1;
         const bool meas = color == 1 && L.every > 0 && ((s + 1) % L.every) == 0;
         Int8Half p;
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
                 y = (int)(row - (long long)z * L.ly);
             }
             for (int jc = tx; jc < p.cpr; jc += bx)
-                int8_chunk<V, NDIM, RULE>(p, row, y, z, jc * V, m_acc, e_acc);
+                int8_chunk<V, NDIM, RULE>(p, row, y, z, jc * V, stab, m_acc, e_acc);
         }
         if (meas) block_accumulate2(m_acc, e_acc, p.meas);
         __syncthreads();

@@ -11,13 +11,12 @@
 // counting is byte-parallel (SWAR): with +1 = 0x01 and -1 = 0xFF, bit 1 of each byte is the
 // "down" flag, so (a ^ b) & 0x02020202 marks anti-aligned pairs of four sites at once.
 //
-// Decision without table lookups.  Metropolis flips iff X <= 0 or u < table[(X + 2d)/2] with
-// X = s*h = 2d - 2A (A = anti-aligned neighbours).  Let T(a) = table[2d - a] for a < d; threshold
-// tables built by threshold_table() make T non-decreasing in a, so with
-// L = #{a < d : u < T(a)} the rule is exactly "flip iff A + L >= d".  Heat bath sets +1 iff
-// u < table[U] (U = up neighbours = 2d - D); with the table non-decreasing and
-// L = #{k <= 2d : u < table[k]} this is "up iff L > D".  Both comparisons run byte-parallel.
-// Tables that are not monotone use the generic per-site lookup rules.
+// Metropolis decision without lookups.  Metropolis flips iff X <= 0 or u < table[(X + 2d)/2]
+// with X = s*h = 2d - 2A (A = anti-aligned neighbours).  Let T(a) = table[2d - a] for a < d;
+// threshold tables built by threshold_table() make T non-decreasing in a, so with
+// L = #{a < d : u < T(a)} the rule is exactly "flip iff A + L >= d", evaluated byte-parallel.
+// Heat bath (+1 iff u < table[U], U = up neighbours = 2d - D) and Metropolis with a table that
+// is not monotone read table[.] per site from a shared-memory copy of the table.
 #pragma once
 
 #include "common.cuh"
@@ -73,23 +72,28 @@ __device__ __forceinline__ void store_words(int8_t* p, const Words<W>& r)
     }
 }
 
-__device__ __forceinline__ u32 table_at(const Int8Half& p, int i)
+// 32-bit load from a shared-memory byte address.
+__device__ __forceinline__ u32 lds_u32(u32 addr)
 {
-    // Constant indices only, so the table stays in the kernel parameter bank.
-    u32 v = p.table[0];
-    v = i == 1 ? p.table[1] : v;
-    v = i == 2 ? p.table[2] : v;
-    v = i == 3 ? p.table[3] : v;
-    v = i == 4 ? p.table[4] : v;
-    v = i == 5 ? p.table[5] : v;
-    v = i == 6 ? p.table[6] : v;
+    u32 v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
     return v;
 }
 
+// 4-bit mask (bit i = site i) -> XOR pattern 0xFE in byte i (the flip of a +-1 byte).
+__device__ __forceinline__ u32 flip_bytes(u32 m4)
+{
+    return ((m4 * 0x00204081u) & 0x01010101u) * 0xFEu;  // bit i -> byte i, then 0x01 -> 0xFE
+}
+
 // New spins of the four sites in word `s` given their anti-aligned (Metropolis) or down
-// (heat bath) neighbour counts `cnt` (one byte per site) and their four uniforms.
+// (heat bath) neighbour counts `cnt` (one byte per site) and their four uniforms.  `stab` is
+// the acceptance table in shared memory (used by the lookup rules).
+//   kMetroFast: byte-parallel "A + #{a<d : u < T(a)} >= d" (monotone Metropolis tables);
+//   heat bath and kMetroGeneric: one shared-memory lookup per site, valid for any table.
 template <int NDIM, int RULE>
-__device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const u32x4& r)
+__device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const u32x4& r,
+                                       const u32* stab)
 {
     constexpr int d = NDIM;
     if constexpr (RULE == kObserve) {
@@ -106,35 +110,24 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
         const u32 lw = l[0] | (l[1] << 8) | (l[2] << 16) | (l[3] << 24);
         const u32 m7 = (cnt + lw + (u32)(0x80 - d) * 0x01010101u) & kBit7;
         return s ^ flip_mask_from_bit7(m7);
-    } else if constexpr (RULE == kHeatFast) {
-        u32 l[4] = {0, 0, 0, 0};
-        const u32 uu[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-        for (int k = 0; k <= 2 * d; ++k) {
-            const u32 thr = p.table[k];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) l[i] += uu[i] < thr ? 1u : 0u;
-        }
-        const u32 lw = l[0] | (l[1] << 8) | (l[2] << 16) | (l[3] << 24);
-        const u32 m7 = (lw + 0x7F7F7F7Fu - cnt) & kBit7;  // up iff L > D
-        return 0xFFFFFFFFu ^ flip_mask_from_bit7(m7);
+    } else if constexpr (RULE == kHeatFast || RULE == kHeatGeneric) {
+        // +1 iff u < table[U], U = up neighbours = 2d - D; rt[k] = table[2d - k]
+        const u32 base = (u32)__cvta_generic_to_shared(stab) + 8u * d;  // &table[2d]
+        const u32 b0 = r.x < lds_u32(base - 4u * (cnt & 0xFFu)) ? 1u : 0u;
+        const u32 b1 = r.y < lds_u32(base - 4u * ((cnt >> 8) & 0xFFu)) ? 2u : 0u;
+        const u32 b2 = r.z < lds_u32(base - 4u * ((cnt >> 16) & 0xFFu)) ? 4u : 0u;
+        const u32 b3 = r.w < lds_u32(base - 4u * (cnt >> 24)) ? 8u : 0u;
+        return 0xFFFFFFFFu ^ flip_bytes(b0 | b1 | b2 | b3);
     } else {
-        const u32 uu[4] = {r.x, r.y, r.z, r.w};
-        u32 out = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int c = (int)((cnt >> (8 * i)) & 0xFFu);
-            const u32 sb = (s >> (8 * i)) & 0xFFu;
-            u32 nb;
-            if constexpr (RULE == kMetroGeneric) {
-                const bool flip = c >= d || uu[i] < table_at(p, 2 * d - c);
-                nb = flip ? (sb ^ 0xFEu) : sb;
-            } else {
-                nb = uu[i] < table_at(p, 2 * d - c) ? 0x01u : 0xFFu;
-            }
-            out |= nb << (8 * i);
-        }
-        return out;
+        // Metropolis, any table: flip iff A >= d or u < table[2d - A]
+        const u32 base = (u32)__cvta_generic_to_shared(stab) + 8u * d;  // &table[2d]
+        const u32 a0 = cnt & 0xFFu, a1 = (cnt >> 8) & 0xFFu, a2 = (cnt >> 16) & 0xFFu,
+                  a3 = cnt >> 24;
+        const u32 f0 = (a0 >= (u32)d || r.x < lds_u32(base - 4u * a0)) ? 1u : 0u;
+        const u32 f1 = (a1 >= (u32)d || r.y < lds_u32(base - 4u * a1)) ? 2u : 0u;
+        const u32 f2 = (a2 >= (u32)d || r.z < lds_u32(base - 4u * a2)) ? 4u : 0u;
+        const u32 f3 = (a3 >= (u32)d || r.w < lds_u32(base - 4u * a3)) ? 8u : 0u;
+        return s ^ flip_bytes(f0 | f1 | f2 | f3);
     }
 }
 
@@ -142,7 +135,7 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
 // `row` = (z, y) of the lattice in p; (M, E) contributions go to m_acc / e_acc when p.meas.
 template <int V, int NDIM, int RULE>
 __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
-                                           long long& m_acc, long long& e_acc)
+                                           const u32* stab, long long& m_acc, long long& e_acc)
 {
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
@@ -179,48 +172,59 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
         }
     }
 
-    Words<W> ns;
-    const u32 q0 = (u32)((unsigned long long)(rb + j0) >> 2);
+    // Neighbour counts first, so the neighbour words are dead before the Philox blocks.
+    u32 cnt[W];
+    int other_down = 0;  // down spins of the opposite colour at the same indices (for M)
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-        u32 cnt;
         if constexpr (kHeat) {
             u32 acc = (c.v[k] & kBit1) + (hz.v[k] & kBit1) + (nu.v[k] & kBit1) +
                       (nd.v[k] & kBit1);
             if constexpr (NDIM == 3) acc += (zu.v[k] & kBit1) + (zd.v[k] & kBit1);
-            cnt = acc >> 1;  // down neighbours per site
+            cnt[k] = acc >> 1;  // down neighbours per site
         } else {
             const u32 sv = s.v[k];
             u32 acc = ((c.v[k] ^ sv) & kBit1) + ((hz.v[k] ^ sv) & kBit1) +
                       ((nu.v[k] ^ sv) & kBit1) + ((nd.v[k] ^ sv) & kBit1);
             if constexpr (NDIM == 3)
                 acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
-            cnt = acc >> 1;  // anti-aligned neighbours per site
+            cnt[k] = acc >> 1;  // anti-aligned neighbours per site
         }
+        other_down += __popc(c.v[k] & kBit1);
+    }
+
+    Words<W> ns;
+    const u32 q0 = (u32)((unsigned long long)(rb + j0) >> 2);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
         if constexpr (RULE == kObserve) {
             ns.v[k] = s.v[k];
         } else {
             const u32x4 r = philox4x32_10(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
-            ns.v[k] = decide4<NDIM, RULE>(p, s.v[k], cnt, r);
+            ns.v[k] = decide4<NDIM, RULE>(p, s.v[k], cnt[k], r, stab);
         }
     }
     if constexpr (RULE != kObserve) store_words<W>(p.own + rb + j0, ns);
 
     if (p.meas) {
-        // Bonds of this colour's sites: s*h = 2d - 2A per site; E = -sum s*h.
+        // Bonds of this colour's sites: s*h = 2d - 2A' per site (A' = anti-aligned neighbours
+        // of the new spin); E = -sum s*h.  A' follows from the counts: a flipped site's
+        // anti-aligned neighbours are the previously aligned ones (2d - A), and for heat bath
+        // A' = D for a +1 site, 2d - D for a -1 site.
+        constexpr u32 k2d = 0x01010101u * (u32)(2 * NDIM);
         int anti = 0, down = 0;
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const u32 sv = ns.v[k];
-            u32 acc = ((c.v[k] ^ sv) & kBit1) + ((hz.v[k] ^ sv) & kBit1) +
-                      ((nu.v[k] ^ sv) & kBit1) + ((nd.v[k] ^ sv) & kBit1);
-            if constexpr (NDIM == 3)
-                acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
-            anti += byte_sum(acc >> 1);
-            down += __popc(sv & kBit1) + __popc(c.v[k] & kBit1);
+            u32 sel;  // 0xFF in the bytes whose count is replaced by 2d - count
+            if constexpr (kHeat) sel = ((sv & kBit1) >> 1) * 0xFFu;
+            else sel = (((sv ^ s.v[k]) & kBit1) >> 1) * 0xFFu;
+            const u32 ap = (cnt[k] & ~sel) | ((k2d - cnt[k]) & sel);
+            anti += byte_sum(ap);
+            down += __popc(sv & kBit1);
         }
-        m_acc += 2 * V - 2 * down;          // this colour's V sites + the other's V
-        e_acc += 2 * anti - 2 * NDIM * V;   // -(2d V - 2 anti)
+        m_acc += 2 * V - 2 * (down + other_down);  // this colour's V sites + the other's V
+        e_acc += 2 * anti - 2 * NDIM * V;          // -(2d V - 2 anti)
     }
 }
 

@@ -7,6 +7,12 @@ namespace ising {
 template <int V, int NDIM, int RULE>
 __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
 {
+    __shared__ u32 stab[8];  // acceptance table for the per-site lookup rules
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) stab[i] = p.table[i];  // constant indices: stays in params
+    }
+    __syncthreads();
     const int jc = blockIdx.x * blockDim.x + threadIdx.x;
     long long m_acc = 0, e_acc = 0;
     if (jc < p.cpr) {
@@ -34,7 +40,7 @@ __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
             } else {
                 y = (int)row;
             }
-            int8_chunk<V, NDIM, RULE>(p, row, y, z, j0, m_acc, e_acc);
+            int8_chunk<V, NDIM, RULE>(p, row, y, z, j0, stab, m_acc, e_acc);
         }
     }
     if (p.meas) block_accumulate2(m_acc, e_acc, p.meas);
