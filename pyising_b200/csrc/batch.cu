@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
         for (int i = 0; i < 7; ++i) p.table[i] = L.table[i];
         p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
                       : nullptr;
+        p.ctl = nullptr;
         const int bx = 1 << L.bx_log2;
         const int tx = threadIdx.x & (bx - 1), ty = threadIdx.x >> L.bx_log2;
         const int by = 256 >> L.bx_log2;
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         p.thr4 = L.table[3];
         p.thr8 = L.table[4];
         p.stats = nullptr;
+        p.ctl = nullptr;
         p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
                       : nullptr;
         if (meas) {

@@ -52,6 +52,75 @@ int select_rule(int variant, int algorithm, int ndim, const u32* table)
 
 }  // namespace ising
 
+namespace ising {
+
+// Sweeps per captured chunk without measurements; longest chunk captured at all.
+constexpr int64_t kGraphChunk = 32;
+constexpr int64_t kGraphChunkMax = 256;
+
+__global__ void ctl_set_kernel(unsigned long long* ctl, unsigned long long t,
+                               unsigned long long k)
+{
+    ctl[0] = t;
+    ctl[1] = k;
+}
+
+__global__ void ctl_advance_kernel(unsigned long long* ctl, unsigned long long dt,
+                                   unsigned long long dk)
+{
+    ctl[0] += dt;
+    ctl[1] += dk;
+}
+
+void clear_graphs(ising_sim* h)
+{
+    for (auto& g : h->graphs) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+}
+
+// The captured chunk of G sweeps of this handle: 2G half-sweeps with counters relative to the
+// control block d_acc[6] (sweep) / d_acc[7] (series slot), then one node advancing it.
+static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* out)
+{
+    for (auto& g : h->graphs)
+        if (g.sweeps == G && g.measured == measured) {
+            *out = g.exec;
+            return ISING_OK;
+        }
+    const unsigned long long* ctl = h->d_acc + 6;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+    int rc = ISING_OK;
+    for (int64_t s = 0; s < G && rc == ISING_OK; ++s) {
+        unsigned long long* m =
+            (measured && s == G - 1) ? (unsigned long long*)h->d_series : nullptr;
+        rc = half_sweep(h, 0, (u32)s, nullptr, nullptr, ctl);
+        if (rc == ISING_OK) rc = half_sweep(h, 1, (u32)s, m, nullptr, ctl);
+    }
+    if (rc == ISING_OK) {
+        ctl_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_acc + 6, (unsigned long long)G,
+                                                   measured ? 1ull : 0ull);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "graph capture");
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc != ISING_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    h->graphs.push_back({G, measured, exec});
+    *out = exec;
+    return ISING_OK;
+}
+
+}  // namespace ising
+
 using namespace ising;
 
 #define TRY_CUDA(call)                                   \
@@ -179,6 +248,7 @@ int ising_destroy(ising_sim* h)
     if (h->d_acc) cudaFree(h->d_acc);
     if (h->d_series) cudaFree(h->d_series);
     if (h->h_series) cudaFreeHost(h->h_series);
+    clear_graphs(h);
     if (h->own_stream_handle) cudaStreamDestroy(h->own_stream_handle);
     cudaGetLastError();
     delete h;
@@ -200,6 +270,7 @@ int ising_set_table(ising_sim* h, const uint32_t* table, int n)
         return fail(ISING_ERR_INVALID, "table must have %d entries, got %d", h->table_n, n);
     for (int i = 0; i < 7; ++i) h->table[i] = i < n ? table[i] : 0xFFFFFFFFu;
     h->rule = select_rule(h->variant, h->algorithm, h->ndim, h->table);
+    clear_graphs(h);  // the table is part of the captured launches
     return ISING_OK;
 }
 
@@ -207,6 +278,7 @@ int ising_set_seed(ising_sim* h, uint64_t seed)
 {
     CHECK_HANDLE(h);
     h->seed = seed;
+    clear_graphs(h);
     return ISING_OK;
 }
 
@@ -342,8 +414,22 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
         TRY_CUDA(cudaMemsetAsync(h->d_series, 0, (size_t)n_meas * 2 * sizeof(long long),
                                  h->stream));
     }
-    int64_t k = 0;
-    for (int64_t s = 0; s < n_sweeps; ++s) {
+    int64_t k = 0, s0 = 0;
+    // Whole chunks of G sweeps replay one captured graph (G = the measurement interval, so each
+    // chunk ends with its measurement); the rest is launched directly.
+    const int64_t G = measure_every > 0 ? measure_every : kGraphChunk;
+    if (G <= kGraphChunkMax && n_sweeps >= 2 * G) {
+        cudaGraphExec_t exec = nullptr;
+        int rc = chunk_graph(h, G, measure_every > 0, &exec);
+        if (rc != ISING_OK) return rc;
+        ctl_set_kernel<<<1, 1, 0, h->stream>>>(h->d_acc + 6, t0, 0);
+        TRY_CUDA(cudaGetLastError());
+        const int64_t chunks = n_sweeps / G;
+        for (int64_t c = 0; c < chunks; ++c) TRY_CUDA(cudaGraphLaunch(exec, h->stream));
+        s0 = chunks * G;
+        k = measure_every > 0 ? chunks : 0;
+    }
+    for (int64_t s = s0; s < n_sweeps; ++s) {
         const u32 t = (u32)(t0 + (uint64_t)s);
         const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;
         unsigned long long* m = meas ? (unsigned long long*)(h->d_series + 2 * k) : nullptr;
@@ -483,6 +569,7 @@ namespace ising {
 int ensure_series(ising_sim* h, int64_t pairs)
 {
     if (pairs <= h->series_cap) return ISING_OK;
+    clear_graphs(h);  // captured measured chunks point into the old buffer
     if (h->d_series) cudaFree(h->d_series);
     if (h->h_series) cudaFreeHost(h->h_series);
     h->d_series = nullptr;
@@ -504,7 +591,7 @@ int ensure_series(ising_sim* h, int64_t pairs)
 }
 
 int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
-               unsigned long long* stats)
+               unsigned long long* stats, const unsigned long long* ctl)
 {
     const u32 k0 = (u32)h->seed, k1 = (u32)(h->seed >> 32);
     cudaError_t e;
@@ -522,6 +609,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.thr8 = h->table[4];
         p.meas = meas;
         p.stats = stats;
+        p.ctl = ctl;
         e = launch_msc_half(true, p, h->max_blocks, h->stream);
     } else {
         Int8Half p;
@@ -538,6 +626,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.k1 = k1;
         for (int i = 0; i < 7; ++i) p.table[i] = h->table[i];
         p.meas = meas;
+        p.ctl = ctl;
         e = launch_int8_half(h->ndim, h->rule, p, h->max_blocks, h->stream);
     }
     if (e != cudaSuccess) return cuda_fail(e, "half-sweep launch");

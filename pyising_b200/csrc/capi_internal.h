@@ -2,6 +2,7 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "ising_b200.h"
@@ -32,6 +33,14 @@ struct ising_sim {
     int64_t series_cap = 0;               // pairs
     int sm_count = 148;
     int max_blocks = 148 * 8;
+    // Captured chunks of `sweeps` sweeps (one measurement at the end when `measured`), replayed
+    // with the sweep counter and series slot in d_acc[6], d_acc[7].
+    struct Graph {
+        int64_t sweeps;
+        bool measured;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
 };
 
 namespace ising {
@@ -44,7 +53,8 @@ int select_rule(int variant, int algorithm, int ndim, const u32* table);
 
 int ensure_series(ising_sim* h, int64_t pairs);
 int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
-               unsigned long long* stats);
+               unsigned long long* stats, const unsigned long long* ctl = nullptr);
+void clear_graphs(ising_sim* h);
 int observe(ising_sim* h, unsigned long long* acc);
 
 // kernel launchers

@@ -115,6 +115,9 @@ struct Int8Half {
     u32 k0, k1;  // Philox key (seed lo, hi)
     u32 table[7];
     unsigned long long* meas;  // (M, E) accumulators, or nullptr
+    // Graph-replay control block, or nullptr: when set, the sweep counter is ctl[0] + t and the
+    // accumulators are meas + 2 * ctl[1] (a captured chunk of sweeps advances ctl itself).
+    const unsigned long long* ctl;
 };
 
 // Parameters of one packed (msc) half-sweep launch over (rows, nw) uint64 words.
@@ -128,6 +131,17 @@ struct MscHalf {
     u32 thr8;   // table[4]: acceptance for none (dE = 8)
     unsigned long long* meas;   // (M, E) accumulators, or nullptr
     unsigned long long* stats;  // (calls, warp-max calls) diagnostics, or nullptr
+    const unsigned long long* ctl;  // graph-replay control block, as in Int8Half
 };
+
+// Resolve the graph-replay control block of a launch (see Int8Half::ctl).
+template <typename P>
+__device__ __forceinline__ void resolve_ctl(P& p)
+{
+    if (p.ctl) {
+        p.t += (u32)p.ctl[0];
+        if (p.meas) p.meas += 2 * p.ctl[1];
+    }
+}
 
 }  // namespace ising

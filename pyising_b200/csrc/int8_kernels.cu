@@ -5,8 +5,10 @@
 namespace ising {
 
 template <int V, int NDIM, int RULE>
-__global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p)
+__global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
 {
+    Int8Half p = p_in;
+    resolve_ctl(p);
     __shared__ u32 stab[8];  // acceptance table for the per-site lookup rules
     if (threadIdx.x == 0 && threadIdx.y == 0) {
 #pragma unroll

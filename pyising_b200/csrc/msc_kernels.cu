@@ -10,8 +10,10 @@
 namespace ising {
 
 template <bool UPDATE>
-__global__ void __launch_bounds__(256) msc_half_kernel(const MscHalf p)
+__global__ void __launch_bounds__(256) msc_half_kernel(const MscHalf p_in)
 {
+    MscHalf p = p_in;
+    resolve_ctl(p);
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     long long m_acc = 0, e_acc = 0;
     long long calls_acc = 0, wmax_acc = 0;
@@ -27,8 +29,10 @@ __global__ void __launch_bounds__(256) msc_half_kernel(const MscHalf p)
 constexpr int kQueueWarps = 8;
 
 __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
-    msc_half_queue_kernel(const MscHalf p, long long total, long long per_warp, int nw_shift)
+    msc_half_queue_kernel(const MscHalf p_in, long long total, long long per_warp, int nw_shift)
 {
+    MscHalf p = p_in;
+    resolve_ctl(p);
     __shared__ QueueSlots q_all[kQueueWarps];
     __shared__ uint4 lvmask[16];
     if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);

@@ -147,6 +147,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 p.thr8 = tab[4];
                 p.meas = m;
                 p.stats = nullptr;
+                p.ctl = nullptr;
                 e = launch_msc_half(true, p, max_blocks, st);
             } else {
                 Int8Half p;
@@ -163,6 +164,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 p.k1 = k1;
                 for (int i = 0; i < 7; ++i) p.table[i] = tab[i];
                 p.meas = m;
+                p.ctl = nullptr;
                 e = launch_int8_half(ndim, rule, p, max_blocks, st);
             }
             if (e != cudaSuccess) return cuda_fail(e, "static sweep launch");
