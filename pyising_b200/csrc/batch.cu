@@ -44,6 +44,10 @@ struct BatchLattice {
     u32 table[7];
 };
 
+// Work-item sizes: ~64K int8 sites (whole rows) or 16K packed words (2K per warp).
+constexpr long long kInt8ItemSites = 65536;
+constexpr long long kMscItemWords = 16384;
+
 struct BatchItem {
     int lat;
     int pad;
@@ -481,8 +485,9 @@ private:
             const int li = (int)lats.size();
             if (s.variant == ISING_VARIANT_MSC) {
                 const long long words = (long long)j.rows * j.nw;
-                for (long long b = 0; b < words; b += 4096)
-                    by_class[kc].push_back(BatchItem{li, 0, b, std::min(words, b + 4096)});
+                for (long long b = 0; b < words; b += kMscItemWords)
+                    by_class[kc].push_back(
+                        BatchItem{li, 0, b, std::min(words, b + kMscItemWords)});
             } else {
                 const int v = int8_chunk_width(j.lh);
                 L.cpr = j.lh / v;
@@ -491,7 +496,7 @@ private:
                 L.bx_log2 = __builtin_ctz((unsigned)bx);
                 kc.v = v;
                 kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
-                long long rpi = 16384 / j.lh;
+                long long rpi = kInt8ItemSites / j.lh;
                 if (rpi < 1) rpi = 1;
                 for (long long b = 0; b < j.rows; b += rpi)
                     by_class[kc].push_back(BatchItem{li, 0, b, std::min<long long>(j.rows, b + rpi)});
@@ -639,10 +644,12 @@ private:
         return ISING_OK;
     }
 
-    // Keeps the host at most kMaxAhead sweeps ahead of the device.
+    // Records the end of the sweep just issued; the host stays at most kMaxAhead sweeps ahead
+    // of the device (see throttle_event), so a newly admitted job starts soon after it joins.
+    static constexpr size_t kMaxAhead = 8;
+
     int throttle()
     {
-        static const size_t kMaxAhead = 64;
         cudaEvent_t ev = nullptr;
         if (!free_events_.empty()) {
             ev = free_events_.back();
@@ -654,14 +661,34 @@ private:
         }
         cudaEventRecord(ev, stream_);
         inflight_.push_back(ev);
-        while (inflight_.size() > kMaxAhead) {
-            cudaError_t e = cudaEventSynchronize(inflight_.front());
+        return ISING_OK;
+    }
+
+public:
+    // The event to wait for before issuing more work (nullptr: not too far ahead).  Callers
+    // wait without holding any lock the submitters need, then call throttle_done().
+    cudaEvent_t throttle_event() const
+    {
+        return inflight_.size() > kMaxAhead ? inflight_.front() : nullptr;
+    }
+
+    void throttle_done()
+    {
+        free_events_.push_back(inflight_.front());
+        inflight_.pop_front();
+    }
+
+    int wait_throttle()
+    {
+        while (cudaEvent_t ev = throttle_event()) {
+            const cudaError_t e = cudaEventSynchronize(ev);
             if (e != cudaSuccess) return cuda_fail(e, "throttle");
-            free_events_.push_back(inflight_.front());
-            inflight_.pop_front();
+            throttle_done();
         }
         return ISING_OK;
     }
+
+private:
 
     void free_job(Job& j, bool shutdown)
     {
@@ -744,6 +771,7 @@ int ising_batch_run(ising_batch* b, int64_t max_epochs, int64_t* epochs_run)
     while (b->eng->has_work() && (max_epochs <= 0 || n < max_epochs)) {
         const size_t before = b->eng->active_count() + b->eng->pending_count();
         int rc = b->eng->step();
+        if (rc == ISING_OK) rc = b->eng->wait_throttle();
         if (rc != ISING_OK) return rc;
         ++n;
         if (b->eng->active_count() == 0 && b->eng->pending_count() > 0 &&
@@ -816,6 +844,18 @@ static void server_loop(ising_server* s)
                     s->error = rc;
                     s->error_msg = g_last_error;
                 }
+            }
+            // bound the run-ahead without holding the lock submitters and waiters need
+            while (cudaEvent_t ev = s->eng->throttle_event()) {
+                lk.unlock();
+                const cudaError_t e = cudaEventSynchronize(ev);
+                lk.lock();
+                if (e != cudaSuccess) {
+                    s->error = cuda_fail(e, "throttle");
+                    s->error_msg = g_last_error;
+                    break;
+                }
+                s->eng->throttle_done();
             }
         } else {
             lk.unlock();

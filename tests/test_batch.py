@@ -192,3 +192,15 @@ def test_server_job_alone_and_in_the_mix_agree():
             srv.wait(f)
     np.testing.assert_array_equal(alone.series, mixed.series)
     np.testing.assert_array_equal(alone.lattice, mixed.lattice)
+
+
+def test_run_sharded_single_process_uses_the_batch(oracle_mod):
+    """World size 1: the default runner is the batched engine on this GPU."""
+    from pyising_b200.distributed import run_sharded
+
+    jobs = mixed_jobs()[:6]
+    res = run_sharded(jobs)
+    for r, job in zip(res, jobs, strict=True):
+        want_series, want_lat = solo(job, oracle_mod)
+        np.testing.assert_array_equal(r.series, want_series)
+        np.testing.assert_array_equal(r.lattice, want_lat)
