@@ -37,6 +37,8 @@ struct BatchLattice {
     int variant;
     int ndim;
     int rows, lh, ly, lz, cpr, nw, nw_shift;
+    int pitch;             // int8: bytes between rows (lh rounded up to 16)
+    u64 nw_magic;          // msc: ceil(2^64 / nw)
     int bx_log2;           // int8: threads along a row = 1 << bx_log2 (of 256)
     int every;             // measurement interval in sweeps (0 = none)
     u32 t0;
@@ -76,6 +78,8 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
         p.ly = L.ly;
         p.lz = L.lz;
         p.cpr = L.cpr;
+        p.pitch = L.pitch;
+        p.vw = V;
         p.t = L.t0 + (u32)s;
         p.color = color;
         p.k0 = L.k0;
@@ -129,6 +133,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         p.k1 = L.k1;
         p.thr4 = L.table[3];
         p.thr8 = L.table[4];
+        p.nw_magic = L.nw_magic;
         p.stats = nullptr;
         p.ctl = nullptr;
         p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
@@ -136,7 +141,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         if (meas) {
             long long m_acc = 0, e_acc = 0, ca = 0, wm = 0;
             for (long long w = item.begin + threadIdx.x; w < item.end; w += blockDim.x) {
-                const int y = (int)(L.nw_shift >= 0 ? (w >> L.nw_shift) : (w / L.nw));
+                const int y = (int)(L.nw_shift >= 0 ? (w >> L.nw_shift) : div_magic(w, p.nw_magic, L.nw));
                 msc_word<true>(p, y, (int)(w - (long long)y * L.nw), m_acc, e_acc, ca, wm);
             }
             block_accumulate2(m_acc, e_acc, p.meas);
@@ -155,8 +160,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
 }
 
 // ----------------------------------------------------------------------------- host engine ---
-cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
-                                int max_blocks, cudaStream_t st);
 
 using Clock = std::chrono::steady_clock;
 
@@ -166,6 +169,7 @@ struct Job {
     ising_job spec;
     std::vector<int8_t> init;  // host copy of an initial lattice (ISING_INIT_LATTICE)
     int rows = 0, lh = 0, ly = 0, lz = 1, nw = 0;
+    int pitch = 0;  // int8: bytes between rows on the device (lh rounded up to 16)
     size_t colour_bytes = 0, series_pairs = 0, device_bytes = 0;
     void* c[2] = {nullptr, nullptr};
     long long* d_series = nullptr;
@@ -376,8 +380,9 @@ private:
         j.ly = (int)ly;
         j.lz = (int)lz;
         j.nw = (int)(lx / 128);
+        j.pitch = (j.lh + 15) / 16 * 16;
         j.colour_bytes = s.variant == ISING_VARIANT_MSC ? (size_t)j.rows * j.nw * 8
-                                                       : (size_t)j.rows * j.lh;
+                                                       : (size_t)j.rows * j.pitch;
         j.series_pairs = s.measure_every > 0 ? (size_t)(s.n_sweeps / s.measure_every) : 0;
         j.device_bytes = 2 * j.colour_bytes + j.series_pairs * 2 * sizeof(long long);
         return ISING_OK;
@@ -418,7 +423,7 @@ private:
             for (int c = 0; c < 2 && e == cudaSuccess; ++c)
                 e = cudaMemsetAsync(j.c[c], v, j.colour_bytes, stream_);
         } else if (s.init == ISING_INIT_PHILOX) {
-            e = launch_philox_start(j.c[0], j.c[1], (long long)j.rows * j.lh,
+            e = launch_philox_start(j.c[0], j.c[1], j.rows, j.lh, j.pitch,
                                     s.variant == ISING_VARIANT_MSC, (u32)s.seed,
                                     (u32)(s.seed >> 32), max_blocks, stream_);
         } else {
@@ -433,7 +438,7 @@ private:
                                         max_blocks, stream_);
                 else
                     e = launch_int8_split(stage, (int8_t*)j.c[0], (int8_t*)j.c[1], j.rows, 0,
-                                          j.lh, j.ly, max_blocks, stream_);
+                                          j.lh, j.pitch, j.ly, max_blocks, stream_);
             }
             if (stage) cudaFreeAsync(stage, stream_);
             std::vector<int8_t>().swap(j.init);
@@ -476,6 +481,7 @@ private:
             L.nw = j.nw;
             L.nw_shift = s.variant == ISING_VARIANT_MSC && (j.nw & (j.nw - 1)) == 0
                              ? __builtin_ctz((unsigned)j.nw) : -1;
+            L.nw_magic = magic_for(j.nw);
             L.every = (int)s.measure_every;
             L.t0 = (u32)s.t0;
             L.k0 = (u32)s.seed;
@@ -489,8 +495,9 @@ private:
                     by_class[kc].push_back(
                         BatchItem{li, 0, b, std::min(words, b + kMscItemWords)});
             } else {
-                const int v = int8_chunk_width(j.lh);
-                L.cpr = j.lh / v;
+                const int v = 16;  // rows padded to 16 bytes
+                L.pitch = j.pitch;
+                L.cpr = (j.lh + v - 1) / v;
                 int bx = 1;
                 while (bx < L.cpr && bx < 128) bx <<= 1;
                 L.bx_log2 = __builtin_ctz((unsigned)bx);
@@ -621,7 +628,7 @@ private:
                                           j.nw, sms_ * 8, stream_);
                 else
                     e = launch_int8_merge((const int8_t*)j.c[0], (const int8_t*)j.c[1], stage,
-                                          j.rows, 0, j.lh, j.ly, sms_ * 8, stream_);
+                                          j.rows, 0, j.lh, j.pitch, j.ly, sms_ * 8, stream_);
             }
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(j.h_lattice, stage, full, cudaMemcpyDeviceToHost, stream_);

@@ -200,6 +200,8 @@ int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uin
     h->ly = (int)ly;
     h->lz = (int)lz;
     h->nw = (int)(lx / 128);
+    h->vw = 16;                        // int8 rows padded to 16 bytes: 128-bit chunks everywhere
+    h->pitch = (h->lh + 15) / 16 * 16;
     h->seed = seed;
     h->table_n = 2 * ndim + 1;
     for (int i = 0; i < 7; ++i) h->table[i] = 0xFFFFFFFFu;
@@ -207,7 +209,7 @@ int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uin
     h->sm_count = device_sm_count(device);
     h->max_blocks = h->sm_count * 8;
     h->colour_bytes = variant == ISING_VARIANT_MSC ? (size_t)rows * h->nw * 8
-                                                  : (size_t)rows * (size_t)h->lh;
+                                                  : (size_t)rows * (size_t)h->pitch;
     cudaError_t e = cudaStreamCreateWithFlags(&h->own_stream_handle, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete h;
@@ -282,6 +284,17 @@ int ising_set_seed(ising_sim* h, uint64_t seed)
     return ISING_OK;
 }
 
+// Bytes of one colour row in host arrays (contiguous) and on the device (pitched for int8).
+static size_t host_row_bytes(const ising_sim* h)
+{
+    return h->variant == ISING_VARIANT_MSC ? (size_t)h->nw * 8 : (size_t)h->lh;
+}
+
+static size_t device_row_bytes(const ising_sim* h)
+{
+    return h->variant == ISING_VARIANT_MSC ? (size_t)h->nw * 8 : (size_t)h->pitch;
+}
+
 // Full lattices move through a bounded device staging buffer, a block of rows at a time.
 static const size_t kStagingBytes = (size_t)256 << 20;
 
@@ -314,9 +327,9 @@ int ising_set_lattice(ising_sim* h, const int8_t* full)
                                     (u64*)h->c[1] + r0 * h->nw, (int)nr, (int)r0, h->nw,
                                     h->max_blocks, h->stream);
             else
-                e = launch_int8_split(stage, (int8_t*)h->c[0] + r0 * h->lh,
-                                      (int8_t*)h->c[1] + r0 * h->lh, nr, r0, h->lh, h->ly,
-                                      h->max_blocks, h->stream);
+                e = launch_int8_split(stage, (int8_t*)h->c[0] + r0 * h->pitch,
+                                      (int8_t*)h->c[1] + r0 * h->pitch, nr, r0, h->lh, h->pitch,
+                                      h->ly, h->max_blocks, h->stream);
         }
         if (e != cudaSuccess) rc = cuda_fail(e, "set_lattice");
     }
@@ -343,8 +356,9 @@ int ising_get_lattice(ising_sim* h, int8_t* full)
                                   (const u64*)h->c[1] + r0 * h->nw, stage, (int)nr, (int)r0,
                                   h->nw, h->max_blocks, h->stream);
         else
-            e = launch_int8_merge((const int8_t*)h->c[0] + r0 * h->lh,
-                                  (const int8_t*)h->c[1] + r0 * h->lh, stage, nr, r0, h->lh,
+            e = launch_int8_merge((const int8_t*)h->c[0] + r0 * h->pitch,
+                                  (const int8_t*)h->c[1] + r0 * h->pitch, stage, nr, r0, h->lh,
+                                  h->pitch,
                                   h->ly, h->max_blocks, h->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(full + r0 * row_bytes, stage, nr * row_bytes,
@@ -362,8 +376,13 @@ int ising_upload(ising_sim* h, const void* c0, const void* c1)
     CHECK_HANDLE(h);
     if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
     TRY_CUDA(cudaSetDevice(h->device));
-    TRY_CUDA(cudaMemcpyAsync(h->c[0], c0, h->colour_bytes, cudaMemcpyHostToDevice, h->stream));
-    TRY_CUDA(cudaMemcpyAsync(h->c[1], c1, h->colour_bytes, cudaMemcpyHostToDevice, h->stream));
+    // host rows are contiguous (width) on the host, `pitch` apart on the device
+    const size_t width = host_row_bytes(h), rows = (size_t)h->rows;
+    const size_t dp = device_row_bytes(h);
+    TRY_CUDA(cudaMemcpy2DAsync(h->c[0], dp, c0, width, width, rows, cudaMemcpyHostToDevice,
+                               h->stream));
+    TRY_CUDA(cudaMemcpy2DAsync(h->c[1], dp, c1, width, width, rows, cudaMemcpyHostToDevice,
+                               h->stream));
     TRY_CUDA(cudaStreamSynchronize(h->stream));
     return ISING_OK;
 }
@@ -373,8 +392,12 @@ int ising_download(ising_sim* h, void* c0, void* c1)
     CHECK_HANDLE(h);
     if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
     TRY_CUDA(cudaSetDevice(h->device));
-    TRY_CUDA(cudaMemcpyAsync(c0, h->c[0], h->colour_bytes, cudaMemcpyDeviceToHost, h->stream));
-    TRY_CUDA(cudaMemcpyAsync(c1, h->c[1], h->colour_bytes, cudaMemcpyDeviceToHost, h->stream));
+    const size_t width = host_row_bytes(h), rows = (size_t)h->rows;
+    const size_t dp = device_row_bytes(h);
+    TRY_CUDA(cudaMemcpy2DAsync(c0, width, h->c[0], dp, width, rows, cudaMemcpyDeviceToHost,
+                               h->stream));
+    TRY_CUDA(cudaMemcpy2DAsync(c1, width, h->c[1], dp, width, rows, cudaMemcpyDeviceToHost,
+                               h->stream));
     TRY_CUDA(cudaStreamSynchronize(h->stream));
     return ISING_OK;
 }
@@ -392,7 +415,7 @@ int ising_fill_philox(ising_sim* h, uint64_t start_seed)
 {
     CHECK_HANDLE(h);
     TRY_CUDA(cudaSetDevice(h->device));
-    TRY_CUDA(launch_philox_start(h->c[0], h->c[1], h->rows * (long long)h->lh,
+    TRY_CUDA(launch_philox_start(h->c[0], h->c[1], h->rows, h->lh, h->pitch,
                                  h->variant == ISING_VARIANT_MSC, (u32)start_seed,
                                  (u32)(start_seed >> 32), h->max_blocks, h->stream));
     return ISING_OK;
@@ -607,6 +630,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.k1 = k1;
         p.thr4 = h->table[3];
         p.thr8 = h->table[4];
+        p.nw_magic = magic_for(h->nw);
         p.meas = meas;
         p.stats = stats;
         p.ctl = ctl;
@@ -619,7 +643,9 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.lh = h->lh;
         p.ly = h->ly;
         p.lz = h->lz;
-        p.cpr = h->lh / int8_chunk_width(h->lh);
+        p.pitch = h->pitch;
+        p.vw = h->vw;
+        p.cpr = (h->lh + h->vw - 1) / h->vw;
         p.t = t;
         p.color = (u32)color;
         p.k0 = k0;
@@ -655,7 +681,9 @@ int observe(ising_sim* h, unsigned long long* acc)
         p.lh = h->lh;
         p.ly = h->ly;
         p.lz = h->lz;
-        p.cpr = h->lh / int8_chunk_width(h->lh);
+        p.pitch = h->pitch;
+        p.vw = h->vw;
+        p.cpr = (h->lh + h->vw - 1) / h->vw;
         p.color = 1;
         p.meas = acc;
         e = launch_int8_half(h->ndim, kObserve, p, h->max_blocks, h->stream);

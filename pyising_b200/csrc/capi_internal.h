@@ -19,6 +19,8 @@ struct ising_sim {
     int ly = 0;          // rows per plane
     int lz = 1;          // planes (1 in 2D)
     int nw = 0;          // packed words per row (msc)
+    int pitch = 0;       // int8: bytes between rows on the device (lh rounded up to 16)
+    int vw = 16;         // int8: chunk width of the kernels
     uint64_t seed = 0;
     uint32_t table[7] = {0, 0, 0, 0, 0, 0, 0};
     int table_n = 5;
@@ -64,15 +66,17 @@ cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_bloc
                              cudaStream_t st);
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st);
 cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,
-                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st);
+                              long long row0, int lh, int pitch, int ly, int max_blocks,
+                              cudaStream_t st);
 cudaError_t launch_int8_merge(const int8_t* c0, const int8_t* c1, int8_t* full, long long rows,
-                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st);
+                              long long row0, int lh, int pitch, int ly, int max_blocks,
+                              cudaStream_t st);
 cudaError_t launch_msc_pack(const int8_t* full, u64* w0, u64* w1, int rows, int row0, int nw,
                             int max_blocks, cudaStream_t st);
 cudaError_t launch_msc_unpack(const u64* w0, const u64* w1, int8_t* full, int rows, int row0,
                               int nw, int max_blocks, cudaStream_t st);
-cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
-                                int max_blocks, cudaStream_t st);
+cudaError_t launch_philox_start(void* c0, void* c1, long long rows, int lh, int pitch, int packed,
+                                u32 k0, u32 k1, int max_blocks, cudaStream_t st);
 cudaError_t launch_philox_probe(u32* out, int blocks, int threads, int calls, u32 k0, u32 k1,
                                 cudaStream_t st);
 cudaError_t launch_philox_range(u32* out, long long n, u32 q0, u32 c1, u32 c2, u32 c3, u32 k0,

@@ -109,7 +109,9 @@ struct Int8Half {
     int lh;      // Lx / 2 (bytes per row)
     int ly;      // rows per z plane
     int lz;      // planes (1 in 2D)
-    int cpr;     // chunks per row = lh / V
+    int cpr;     // chunks per row = ceil(lh / V)
+    int pitch;   // bytes between rows in memory (lh, or lh rounded up to 16 with V = 16)
+    int vw;      // chunk width V: 16, 8 or 4 bytes
     u32 t;       // sweep counter (Philox counter word 1)
     u32 color;   // colour being updated (Philox counter word 2)
     u32 k0, k1;  // Philox key (seed lo, hi)
@@ -129,10 +131,20 @@ struct MscHalf {
     u32 t, color, k0, k1;
     u32 thr4;   // table[3]: acceptance for one anti-aligned neighbour (dE = 4)
     u32 thr8;   // table[4]: acceptance for none (dE = 8)
+    u64 nw_magic;  // ceil(2^64 / nw): w / nw = umulhi64(w, nw_magic) for w < 2^32
     unsigned long long* meas;   // (M, E) accumulators, or nullptr
     unsigned long long* stats;  // (calls, warp-max calls) diagnostics, or nullptr
     const unsigned long long* ctl;  // graph-replay control block, as in Int8Half
 };
+
+// w / d with m = ceil(2^64 / d): for 0 <= w < 2^32 and 1 < d < 2^32 the error of w * m / 2^64
+// is below w / 2^64 < 1/d, so it never crosses the next integer; larger w divide directly.
+__device__ __forceinline__ long long div_magic(long long w, u64 m, int d)
+{
+    return ((u64)w >> 32) ? w / d : (long long)__umul64hi((u64)w, m);
+}
+
+inline u64 magic_for(int d) { return d > 1 ? ~0ull / (u64)d + 1ull : 0ull; }
 
 // Resolve the graph-replay control block of a launch (see Int8Half::ctl).
 template <typename P>

@@ -140,31 +140,34 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
     const int par = (y + z + (int)p.color) & 1;
-    const long long rb = row * p.lh;
+    // Rows are `pitch` bytes apart; a row's last chunk may hold fewer than W valid words (the
+    // rest is padding, loaded but never updated, counted or used as a neighbour).
+    const int wv = (p.lh - j0 >= V) ? W : ((p.lh - j0) >> 2);
+    const long long rb = row * p.pitch;
     const int8_t* orow = p.other + rb;
 
     const Words<W> s = load_words<W>(p.own + rb + j0);
     const Words<W> c = load_words_ro<W>(orow + j0);
     const int yu = z * p.ly + (y + 1 == p.ly ? 0 : y + 1);
     const int yd = z * p.ly + (y == 0 ? p.ly - 1 : y - 1);
-    const Words<W> nu = load_words_ro<W>(p.other + (long long)yu * p.lh + j0);
-    const Words<W> nd = load_words_ro<W>(p.other + (long long)yd * p.lh + j0);
+    const Words<W> nu = load_words_ro<W>(p.other + (long long)yu * p.pitch + j0);
+    const Words<W> nd = load_words_ro<W>(p.other + (long long)yd * p.pitch + j0);
     Words<W> zu, zd;
     if constexpr (NDIM == 3) {
         const int pu = (z + 1 == p.lz ? 0 : z + 1) * p.ly + y;
         const int pd = (z == 0 ? p.lz - 1 : z - 1) * p.ly + y;
-        zu = load_words_ro<W>(p.other + (long long)pu * p.lh + j0);
-        zd = load_words_ro<W>(p.other + (long long)pd * p.lh + j0);
+        zu = load_words_ro<W>(p.other + (long long)pu * p.pitch + j0);
+        zd = load_words_ro<W>(p.other + (long long)pd * p.pitch + j0);
     }
-    // horizontal neighbour byte outside this chunk (periodic in x)
-    const int je = par ? (j0 + V == p.lh ? 0 : j0 + V) : (j0 == 0 ? p.lh - 1 : j0 - 1);
+    // horizontal neighbour byte outside this chunk's valid sites (periodic in x)
+    const int je = par ? (j0 + 4 * wv == p.lh ? 0 : j0 + 4 * wv) : (j0 == 0 ? p.lh - 1 : j0 - 1);
     const u32 edge = (u32)(uint8_t)__ldg(orow + je);
 
     Words<W> hz;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
         if (par) {
-            const u32 nx = (k + 1 < W) ? c.v[(k + 1) % W] : edge;
+            const u32 nx = (k + 1 < W && k + 1 < wv) ? c.v[(k + 1) % W] : edge;
             hz.v[k] = __funnelshift_r(c.v[k], nx, 8);
         } else {
             const u32 pv = (k > 0) ? c.v[(k + W - 1) % W] : (edge << 24);
@@ -190,14 +193,15 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
                 acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
             cnt[k] = acc >> 1;  // anti-aligned neighbours per site
         }
-        other_down += __popc(c.v[k] & kBit1);
+        if (k < wv) other_down += __popc(c.v[k] & kBit1);
     }
 
     Words<W> ns;
-    const u32 q0 = (u32)((unsigned long long)(rb + j0) >> 2);
+    // Philox counters use the logical site index row*lh + j, independent of the pitch
+    const u32 q0 = (u32)((unsigned long long)(row * p.lh + j0) >> 2);
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-        if constexpr (RULE == kObserve) {
+        if (RULE == kObserve || k >= wv) {
             ns.v[k] = s.v[k];
         } else {
             const u32x4 r = philox4x32_10(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
@@ -215,6 +219,7 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
         int anti = 0, down = 0;
 #pragma unroll
         for (int k = 0; k < W; ++k) {
+            if (k >= wv) continue;
             const u32 sv = ns.v[k];
             u32 sel;  // 0xFF in the bytes whose count is replaced by 2d - count
             if constexpr (kHeat) sel = ((sv & kBit1) >> 1) * 0xFFu;
@@ -223,8 +228,9 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
             anti += byte_sum(ap);
             down += __popc(sv & kBit1);
         }
-        m_acc += 2 * V - 2 * (down + other_down);  // this colour's V sites + the other's V
-        e_acc += 2 * anti - 2 * NDIM * V;          // -(2d V - 2 anti)
+        const int nv = 4 * wv;                      // valid sites of this chunk
+        m_acc += 2 * nv - 2 * (down + other_down);  // this colour's sites + the other's
+        e_acc += 2 * anti - 2 * NDIM * nv;          // -(2d n - 2 anti)
     }
 }
 

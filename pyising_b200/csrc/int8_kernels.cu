@@ -99,7 +99,7 @@ cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_bloc
 {
     dim3 grid, block;
     int8_geometry(p.rows, p.cpr, max_blocks, &grid, &block);
-    const int v = p.lh / p.cpr;
+    const int v = p.vw;
     if (v == 16) return launch_v<16>(ndim, rule, p, grid, block, st);
     if (v == 8) return launch_v<8>(ndim, rule, p, grid, block, st);
     return launch_v<4>(ndim, rule, p, grid, block, st);

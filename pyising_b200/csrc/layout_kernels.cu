@@ -13,7 +13,7 @@ namespace ising {
 // full (rows, 2*lh) -> c0, c1 (rows, lh); one thread per 4 compressed sites of both colours.
 __global__ void int8_split_kernel(const int8_t* __restrict__ full, int8_t* __restrict__ c0,
                                   int8_t* __restrict__ c1, long long rows, long long row0,
-                                  int lh, int ly)
+                                  int lh, int pitch, int ly)
 {
     const int qpr = lh / 4;
     const long long total = rows * qpr;
@@ -27,14 +27,14 @@ __global__ void int8_split_kernel(const int8_t* __restrict__ full, int8_t* __res
         const uint2 v = *reinterpret_cast<const uint2*>(full + row * 2 * lh + 8 * q);
         const u32 even = __byte_perm(v.x, v.y, 0x6420);
         const u32 odd = __byte_perm(v.x, v.y, 0x7531);
-        *reinterpret_cast<u32*>(c0 + row * lh + 4 * q) = rp ? odd : even;
-        *reinterpret_cast<u32*>(c1 + row * lh + 4 * q) = rp ? even : odd;
+        *reinterpret_cast<u32*>(c0 + row * pitch + 4 * q) = rp ? odd : even;
+        *reinterpret_cast<u32*>(c1 + row * pitch + 4 * q) = rp ? even : odd;
     }
 }
 
 __global__ void int8_merge_kernel(const int8_t* __restrict__ c0, const int8_t* __restrict__ c1,
                                   int8_t* __restrict__ full, long long rows, long long row0,
-                                  int lh, int ly)
+                                  int lh, int pitch, int ly)
 {
     const int qpr = lh / 4;
     const long long total = rows * qpr;
@@ -45,8 +45,8 @@ __global__ void int8_merge_kernel(const int8_t* __restrict__ c0, const int8_t* _
         const long long ar = row0 + row;
         const int y = (int)(ar % ly), z = (int)(ar / ly);
         const int rp = (y + z) & 1;
-        const u32 a = *reinterpret_cast<const u32*>(c0 + row * lh + 4 * q);
-        const u32 b = *reinterpret_cast<const u32*>(c1 + row * lh + 4 * q);
+        const u32 a = *reinterpret_cast<const u32*>(c0 + row * pitch + 4 * q);
+        const u32 b = *reinterpret_cast<const u32*>(c1 + row * pitch + 4 * q);
         const u32 e = rp ? b : a;  // sites at even x
         const u32 o = rp ? a : b;  // sites at odd x
         uint2 v;
@@ -104,48 +104,62 @@ __global__ void msc_unpack_kernel(const u64* __restrict__ w0, const u64* __restr
     }
 }
 
+static unsigned grid_for(long long total, int threads, int max_blocks);
+
 // Device seeded start (not in the reference, whose hot start is NumPy's PCG64): compressed site
 // n of colour c is +1 iff bit n % 32 of word (n / 32) % 4 of Philox((n / 128, 0, c, 0xFFFFFFFF),
 // seed) is set.  Counter word 3 = 0xFFFFFFFF is never used by a sweep, and int8 and packed
-// layouts get the same spins.  One thread per colour and 128-site group; `sites` = sites per
-// colour (rows * Lx/2).
-__global__ void philox_start_kernel(void* c0, void* c1, long long sites, int packed, u32 k0,
-                                    u32 k1)
+// layouts get the same spins.  n is the logical index row * lh + j whatever the row pitch.
+__global__ void philox_start_int8_kernel(int8_t* c0, int8_t* c1, long long rows, int lh,
+                                         int pitch, u32 k0, u32 k1)
 {
-    const long long groups = (sites + 127) / 128;
+    const int qpr = lh / 4;  // 4-site quads per row (lh % 4 == 0)
+    const long long quads = rows * qpr;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < 2 * quads;
+         i += (long long)gridDim.x * blockDim.x) {
+        const u32 color = (u32)(i / quads);
+        const long long qi = i - (long long)color * quads;
+        const long long row = qi / qpr;
+        const int q = (int)(qi - row * qpr);
+        const long long n = row * lh + 4LL * q;
+        const u32x4 r = philox4x32_10((u32)(n >> 7), 0u, color, 0xFFFFFFFFu, k0, k1);
+        const int word = (int)((n >> 5) & 3);
+        const u32 rw = word == 0 ? r.x : (word == 1 ? r.y : (word == 2 ? r.z : r.w));
+        const u32 nib = (rw >> (n & 31)) & 0xFu;
+        const u32 ones = (nib * 0x00204081u) & 0x01010101u;  // bit i -> byte i
+        int8_t* dst = (color ? c1 : c0) + row * pitch + 4 * q;
+        *reinterpret_cast<u32*>(dst) = 0xFFFFFFFFu ^ (ones * 0xFEu);  // 1 -> +1, 0 -> -1
+    }
+}
+
+// Packed layout: words 2g, 2g+1 of a colour come from call g (sites 128g .. 128g + 127).
+__global__ void philox_start_msc_kernel(u64* w0, u64* w1, long long words, u32 k0, u32 k1)
+{
+    const long long groups = words / 2;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < 2 * groups;
          i += (long long)gridDim.x * blockDim.x) {
         const u32 color = (u32)(i / groups);
         const long long g = i - (long long)color * groups;
         const u32x4 r = philox4x32_10((u32)g, 0u, color, 0xFFFFFFFFu, k0, k1);
-        const u32 rw[4] = {r.x, r.y, r.z, r.w};
-        void* dst = color ? c1 : c0;
-        if (packed) {  // words 2g and 2g+1 (sites is a multiple of 128 for the packed layout)
-            u64* w = static_cast<u64*>(dst) + 2 * g;
-            w[0] = (u64)r.x | ((u64)r.y << 32);
-            w[1] = (u64)r.z | ((u64)r.w << 32);
-        } else {
-            int8_t* b = static_cast<int8_t*>(dst) + 128 * g;
-            const long long left = sites - 128 * g;
-            for (int m = 0; m < 32; ++m) {  // 4 sites per m: bits 4m'..4m'+3 of one word
-                if (4 * m >= left) break;
-                const u32 nib = (rw[m >> 3] >> (4 * (m & 7))) & 0xFu;
-                const u32 ones = (nib * 0x00204081u) & 0x01010101u;  // bit i -> byte i
-                const u32 v = 0xFFFFFFFFu ^ (ones * 0xFEu);           // 1 -> +1, 0 -> -1
-                reinterpret_cast<u32*>(b)[m] = v;
-            }
-        }
+        u64* w = (color ? w1 : w0) + 2 * g;
+        w[0] = (u64)r.x | ((u64)r.y << 32);
+        w[1] = (u64)r.z | ((u64)r.w << 32);
     }
 }
 
-cudaError_t launch_philox_start(void* c0, void* c1, long long sites, int packed, u32 k0, u32 k1,
-                                int max_blocks, cudaStream_t st)
+// rows x lh sites per colour (int8, rows `pitch` bytes apart) or rows x nw words (packed).
+cudaError_t launch_philox_start(void* c0, void* c1, long long rows, int lh, int pitch, int packed,
+                                u32 k0, u32 k1, int max_blocks, cudaStream_t st)
 {
-    const long long work = 2 * ((sites + 127) / 128);
-    long long g = (work + 255) / 256;
-    if (g > max_blocks) g = max_blocks;
-    if (g < 1) g = 1;
-    philox_start_kernel<<<(unsigned)g, 256, 0, st>>>(c0, c1, sites, packed, k0, k1);
+    if (packed) {
+        const long long words = rows * (lh / 64);
+        philox_start_msc_kernel<<<grid_for(words, 256, max_blocks), 256, 0, st>>>(
+            static_cast<u64*>(c0), static_cast<u64*>(c1), words, k0, k1);
+    } else {
+        const long long work = 2 * rows * (lh / 4);
+        philox_start_int8_kernel<<<grid_for(work, 256, max_blocks), 256, 0, st>>>(
+            static_cast<int8_t*>(c0), static_cast<int8_t*>(c1), rows, lh, pitch, k0, k1);
+    }
     return cudaGetLastError();
 }
 
@@ -182,20 +196,22 @@ static unsigned grid_for(long long total, int threads, int max_blocks)
 }
 
 cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,
-                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st)
+                              long long row0, int lh, int pitch, int ly, int max_blocks,
+                              cudaStream_t st)
 {
     const long long total = rows * (lh / 4);
     int8_split_kernel<<<grid_for(total, 256, max_blocks), 256, 0, st>>>(full, c0, c1, rows,
-                                                                        row0, lh, ly);
+                                                                        row0, lh, pitch, ly);
     return cudaGetLastError();
 }
 
 cudaError_t launch_int8_merge(const int8_t* c0, const int8_t* c1, int8_t* full, long long rows,
-                              long long row0, int lh, int ly, int max_blocks, cudaStream_t st)
+                              long long row0, int lh, int pitch, int ly, int max_blocks,
+                              cudaStream_t st)
 {
     const long long total = rows * (lh / 4);
     int8_merge_kernel<<<grid_for(total, 256, max_blocks), 256, 0, st>>>(c0, c1, full, rows,
-                                                                        row0, lh, ly);
+                                                                        row0, lh, pitch, ly);
     return cudaGetLastError();
 }
 

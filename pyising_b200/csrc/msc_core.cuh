@@ -154,6 +154,7 @@ __device__ __forceinline__ void call_levels(const u32x4& r, const uint4& m, u32 
 // Global words of one intake batch (one per lane), loaded ahead of use.
 struct IntakeLoads {
     u64 o, c, side, up, dn;
+    int y;  // row of the word
 };
 
 __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool valid, int nw,
@@ -161,6 +162,7 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
 {
     if (!valid) {
         L.o = L.c = L.side = L.up = L.dn = 0;
+        L.y = 0;
         return;
     }
     int y, x;
@@ -168,9 +170,10 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
         y = (int)(w >> nw_shift);
         x = (int)(w & (nw - 1));
     } else {
-        y = (int)(w / nw);
+        y = (int)div_magic(w, p.nw_magic, nw);
         x = (int)(w - (long long)y * nw);
     }
+    L.y = y;
     const u64* orow = p.other + (long long)y * nw;
     L.o = p.own[w];
     L.c = __ldg(orow + x);
@@ -200,8 +203,7 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             const bool valid = w < end;
             u32 a1l = 0, a1h = 0, undl = 0, undh = 0, resl = 0, resh = 0;
             if (valid) {
-                const int yw = (int)(nw_shift >= 0 ? (w >> nw_shift) : (w / nw));
-                const bool par = (yw + (int)p.color) & 1;
+                const bool par = (L.y + (int)p.color) & 1;
                 const u64 hz = par ? ((L.c >> 1) | (L.side << 63)) : ((L.c << 1) | (L.side >> 63));
                 const Slices s = slice4(L.o, L.c, hz, L.up, L.dn);
                 a1l = (u32)s.a1;

@@ -145,6 +145,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 p.k1 = k1;
                 p.thr4 = tab[3];
                 p.thr8 = tab[4];
+                p.nw_magic = magic_for(p.nw);
                 p.meas = m;
                 p.stats = nullptr;
                 p.ctl = nullptr;
@@ -157,7 +158,9 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 p.lh = (int)(lx / 2);
                 p.ly = (int)ly;
                 p.lz = (int)lz;
-                p.cpr = p.lh / int8_chunk_width(p.lh);
+                p.vw = int8_chunk_width(p.lh);  // caller arrays are contiguous: V divides lh
+                p.pitch = p.lh;
+                p.cpr = p.lh / p.vw;
                 p.t = t;
                 p.color = (u32)color;
                 p.k0 = k0;
