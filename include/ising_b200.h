@@ -104,6 +104,22 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
  * src/pyising/backends/cupy_backend.py:68-72,125-135). */
 int ising_half_sweep(ising_sim* h, int color, uint64_t t);
 
+/* How ising_sweep issues its half-sweeps (no counterpart in the reference, which launches one
+ * kernel per half-sweep from Python):
+ *   ISING_SCHEDULE_AUTO       graphs for whole chunks of sweeps, launches for the rest;
+ *   ISING_SCHEDULE_LAUNCHES   one kernel launch per half-sweep;
+ *   ISING_SCHEDULE_GRAPHS     replayed CUDA graphs of whole chunks of sweeps;
+ *   ISING_SCHEDULE_PERSISTENT one cooperative launch for all sweeps (2D int8; others fall back):
+ *                             bands of rows wait only for their neighbours, every wait bounded.
+ * All schedules give identical results.  test_mute_band >= 0 makes that band of a persistent
+ * run stop publishing its progress, so its neighbours' bounded waits expire: the sweep then
+ * reports ISING_ERR_TIMEOUT (the lattice is no longer valid); pass -1 otherwise. */
+#define ISING_SCHEDULE_AUTO 0
+#define ISING_SCHEDULE_LAUNCHES 1
+#define ISING_SCHEDULE_GRAPHS 2
+#define ISING_SCHEDULE_PERSISTENT 3
+int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
+
 /* Exact magnetisation M = sum s and energy E = -sum_<ij> s_i s_j (blocks until done).
  * Replaces: observables / magnetization / energy (src/pyising/backends/base.py:125-135;
  * src/pyising/backends/observables_torch.py:46-111). */
@@ -214,6 +230,11 @@ int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int6
 int ising_server_destroy(ising_server* s);
 
 /* ---- device probes (roofline ceilings and generator checks) ---------------------------- */
+
+/* Self-test of the bounded device-side wait used by the persistent schedule: one CTA waits for
+ * a flag that nothing sets, gives up after ~1 ms and records the time-out; *timed_out = 1 when
+ * that happened and the context is still usable. */
+int ising_selftest_bounded_wait(int device, int* timed_out);
 
 /* Philox4x32-10 throughput of this device in calls/ns (best of `repeats`).
  * Replaces: bench/roofline.py:59-78 (philox_rate). */

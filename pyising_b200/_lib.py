@@ -47,6 +47,8 @@ SIGNATURES: dict[str, tuple] = {
     "ising_msc_calls_per_word": (I, [P, U64, I64, PD, PD]),
     "ising_sweep_static": (I, [I, PI64, I, I, U64, P, I, P, P, U64, I64, I64, P, P]),
     "ising_fill_philox": (I, [P, U64]),
+    "ising_set_schedule": (I, [P, I, I]),
+    "ising_selftest_bounded_wait": (I, [I, ctypes.POINTER(I)]),
     "ising_batch_create": (I, [I, I64, ctypes.POINTER(P)]),
     "ising_batch_add": (I, [P, P, PI64]),
     "ising_batch_run": (I, [P, I64, PI64]),

@@ -58,6 +58,22 @@ namespace ising {
 constexpr int64_t kGraphChunk = 32;
 constexpr int64_t kGraphChunkMax = 256;
 
+// Reads the error word of the last persistent run (waits for the handle's stream).
+static int check_pending(ising_sim* h)
+{
+    if (!h->pending_err) return ISING_OK;
+    h->pending_err = false;
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, h->d_flags + h->sm_count, sizeof(int),
+                                    cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "persistent sweep");
+    if (err)
+        return fail(ISING_ERR_TIMEOUT,
+                    "a bounded wait of the persistent sweep expired; the lattice is not valid");
+    return ISING_OK;
+}
+
 __global__ void ctl_set_kernel(unsigned long long* ctl, unsigned long long t,
                                unsigned long long k)
 {
@@ -251,6 +267,7 @@ int ising_destroy(ising_sim* h)
     if (h->d_series) cudaFree(h->d_series);
     if (h->h_series) cudaFreeHost(h->h_series);
     clear_graphs(h);
+    if (h->d_flags) cudaFree(h->d_flags);
     if (h->own_stream_handle) cudaStreamDestroy(h->own_stream_handle);
     cudaGetLastError();
     delete h;
@@ -341,6 +358,10 @@ int ising_set_lattice(ising_sim* h, const int8_t* full)
 int ising_get_lattice(ising_sim* h, int8_t* full)
 {
     CHECK_HANDLE(h);
+    {
+        const int prc = check_pending(h);
+        if (prc != ISING_OK) return prc;
+    }
     if (!full) return fail(ISING_ERR_INVALID, "null lattice");
     TRY_CUDA(cudaSetDevice(h->device));
     const long long rpc = rows_per_chunk(h);
@@ -390,6 +411,10 @@ int ising_upload(ising_sim* h, const void* c0, const void* c1)
 int ising_download(ising_sim* h, void* c0, void* c1)
 {
     CHECK_HANDLE(h);
+    {
+        const int prc = check_pending(h);
+        if (prc != ISING_OK) return prc;
+    }
     if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
     TRY_CUDA(cudaSetDevice(h->device));
     const size_t width = host_row_bytes(h), rows = (size_t)h->rows;
@@ -421,10 +446,30 @@ int ising_fill_philox(ising_sim* h, uint64_t start_seed)
     return ISING_OK;
 }
 
+int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band)
+{
+    CHECK_HANDLE(h);
+    if (schedule < ISING_SCHEDULE_AUTO || schedule > ISING_SCHEDULE_PERSISTENT)
+        return fail(ISING_ERR_INVALID, "unknown schedule %d", schedule);
+    h->schedule = schedule;
+    h->mute_band = test_mute_band;
+    return ISING_OK;
+}
+
+int ising_selftest_bounded_wait(int device, int* timed_out)
+{
+    if (!timed_out) return fail(ISING_ERR_INVALID, "null output pointer");
+    return selftest_bounded_wait(device, timed_out);
+}
+
 int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
                 int64_t* series_out)
 {
     CHECK_HANDLE(h);
+    {
+        int rc = check_pending(h);
+        if (rc != ISING_OK) return rc;
+    }
     if (n_sweeps < 0) return fail(ISING_ERR_INVALID, "negative sweep count");
     if (measure_every < 0) return fail(ISING_ERR_INVALID, "negative measurement interval");
     if (measure_every > 0 && !series_out)
@@ -438,10 +483,42 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
                                  h->stream));
     }
     int64_t k = 0, s0 = 0;
+    // Small 2D int8 lattices: all sweeps in one persistent cooperative launch.
+    const bool persistent_ok = h->variant == ISING_VARIANT_INT8 && h->ndim == 2 &&
+                               n_sweeps > 0 && n_sweeps < (1LL << 30);
+    // (The automatic schedule uses graphs: on B200 the per-half-sweep chain of flag, halo
+    // reads and fence of the persistent kernel measured 1.7x slower than replayed graphs.)
+    const bool want_persistent = h->schedule == ISING_SCHEDULE_PERSISTENT;
+    if (persistent_ok && want_persistent) {
+        if (!h->d_flags) {
+            cudaError_t e = cudaMalloc(&h->d_flags, (h->sm_count + 2) * sizeof(unsigned int));
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return fail(ISING_ERR_NOMEM, "cudaMalloc of the persistent progress flags");
+            }
+        }
+        int* err = reinterpret_cast<int*>(h->d_flags + h->sm_count);
+        int rc = run_persistent_int8(h, t0, n_sweeps, measure_every,
+                                     n_meas > 0 ? (unsigned long long*)h->d_series : nullptr,
+                                     h->d_flags, err, h->mute_band);
+        if (rc == ISING_OK) {
+            h->pending_err = true;
+            if (n_meas > 0) {
+                TRY_CUDA(cudaMemcpyAsync(h->h_series, h->d_series,
+                                         (size_t)n_meas * 2 * sizeof(long long),
+                                         cudaMemcpyDeviceToHost, h->stream));
+                rc = check_pending(h);
+                if (rc != ISING_OK) return rc;
+                memcpy(series_out, h->h_series, (size_t)n_meas * 2 * sizeof(long long));
+            }
+            return ISING_OK;
+        }
+        if (rc != ISING_ERR_STATE) return rc;  // ISING_ERR_STATE: not resident, fall back
+    }
     // Whole chunks of G sweeps replay one captured graph (G = the measurement interval, so each
     // chunk ends with its measurement); the rest is launched directly.
     const int64_t G = measure_every > 0 ? measure_every : kGraphChunk;
-    if (G <= kGraphChunkMax && n_sweeps >= 2 * G) {
+    if (h->schedule != ISING_SCHEDULE_LAUNCHES && G <= kGraphChunkMax && n_sweeps >= 2 * G) {
         cudaGraphExec_t exec = nullptr;
         int rc = chunk_graph(h, G, measure_every > 0, &exec);
         if (rc != ISING_OK) return rc;
@@ -473,6 +550,10 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
 int ising_half_sweep(ising_sim* h, int color, uint64_t t)
 {
     CHECK_HANDLE(h);
+    {
+        const int prc = check_pending(h);
+        if (prc != ISING_OK) return prc;
+    }
     if (color != 0 && color != 1) return fail(ISING_ERR_INVALID, "colour must be 0 or 1");
     TRY_CUDA(cudaSetDevice(h->device));
     return half_sweep(h, color, (u32)t, nullptr, nullptr);
@@ -481,6 +562,10 @@ int ising_half_sweep(ising_sim* h, int color, uint64_t t)
 int ising_observables(ising_sim* h, int64_t* m, int64_t* e)
 {
     CHECK_HANDLE(h);
+    {
+        const int prc = check_pending(h);
+        if (prc != ISING_OK) return prc;
+    }
     if (!m || !e) return fail(ISING_ERR_INVALID, "null output pointer");
     TRY_CUDA(cudaSetDevice(h->device));
     TRY_CUDA(cudaMemsetAsync(h->d_acc, 0, 2 * sizeof(unsigned long long), h->stream));
@@ -497,6 +582,10 @@ int ising_observables(ising_sim* h, int64_t* m, int64_t* e)
 int ising_sync(ising_sim* h)
 {
     CHECK_HANDLE(h);
+    {
+        const int prc = check_pending(h);
+        if (prc != ISING_OK) return prc;
+    }
     TRY_CUDA(cudaSetDevice(h->device));
     TRY_CUDA(cudaStreamSynchronize(h->stream));
     return ISING_OK;

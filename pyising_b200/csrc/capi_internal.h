@@ -43,6 +43,10 @@ struct ising_sim {
         cudaGraphExec_t exec;
     };
     std::vector<Graph> graphs;
+    int schedule = ISING_SCHEDULE_AUTO;
+    int mute_band = -1;                 // test hook of the persistent schedule
+    unsigned int* d_flags = nullptr;    // persistent schedule: per-band progress + error word
+    bool pending_err = false;           // a persistent run's error word not yet read
 };
 
 namespace ising {
@@ -58,6 +62,9 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
                unsigned long long* stats, const unsigned long long* ctl = nullptr);
 void clear_graphs(ising_sim* h);
 int observe(ising_sim* h, unsigned long long* acc);
+int run_persistent_int8(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
+                        unsigned long long* series, unsigned int* flags, int* err, int mute_band);
+int selftest_bounded_wait(int device, int* timed_out);
 
 // kernel launchers
 int int8_chunk_width(int lh);

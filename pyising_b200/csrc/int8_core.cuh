@@ -60,6 +60,31 @@ __device__ __forceinline__ Words<W> load_words_ro(const int8_t* p)
     return r;
 }
 
+// The opposite colour read from L2, bypassing L1: needed inside one launch that runs several
+// half-sweeps, where other SMs rewrite rows this SM may have cached.
+template <int W>
+__device__ __forceinline__ Words<W> load_words_cg(const int8_t* p)
+{
+    Words<W> r;
+    if constexpr (W == 4) {
+        const uint4 q = __ldcg(reinterpret_cast<const uint4*>(p));
+        r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+    } else if constexpr (W == 2) {
+        const uint2 q = __ldcg(reinterpret_cast<const uint2*>(p));
+        r.v[0] = q.x; r.v[1] = q.y;
+    } else {
+        r.v[0] = __ldcg(reinterpret_cast<const unsigned int*>(p));
+    }
+    return r;
+}
+
+template <int W, bool CG>
+__device__ __forceinline__ Words<W> load_other(const int8_t* p)
+{
+    if constexpr (CG) return load_words_cg<W>(p);
+    else return load_words_ro<W>(p);
+}
+
 template <int W>
 __device__ __forceinline__ void store_words(int8_t* p, const Words<W>& r)
 {
@@ -133,8 +158,8 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
 
 // Update (or, with RULE == kObserve, only measure) the V colour sites starting at j0 in row
 // `row` = (z, y) of the lattice in p; (M, E) contributions go to m_acc / e_acc when p.meas.
-template <int V, int NDIM, int RULE>
-__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
+template <int V, int NDIM, int RULE, bool CG = false, bool FULL = true>
+__device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row, int y, int z, int j0,
                                            const u32* stab, long long& m_acc, long long& e_acc)
 {
     constexpr int W = V / 4;
@@ -142,26 +167,26 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
     const int par = (y + z + (int)p.color) & 1;
     // Rows are `pitch` bytes apart; a row's last chunk may hold fewer than W valid words (the
     // rest is padding, loaded but never updated, counted or used as a neighbour).
-    const int wv = (p.lh - j0 >= V) ? W : ((p.lh - j0) >> 2);
+    const int wv = FULL ? W : ((p.lh - j0 >= V) ? W : ((p.lh - j0) >> 2));
     const long long rb = row * p.pitch;
     const int8_t* orow = p.other + rb;
 
     const Words<W> s = load_words<W>(p.own + rb + j0);
-    const Words<W> c = load_words_ro<W>(orow + j0);
+    const Words<W> c = load_other<W, CG>(orow + j0);
     const int yu = z * p.ly + (y + 1 == p.ly ? 0 : y + 1);
     const int yd = z * p.ly + (y == 0 ? p.ly - 1 : y - 1);
-    const Words<W> nu = load_words_ro<W>(p.other + (long long)yu * p.pitch + j0);
-    const Words<W> nd = load_words_ro<W>(p.other + (long long)yd * p.pitch + j0);
+    const Words<W> nu = load_other<W, CG>(p.other + (long long)yu * p.pitch + j0);
+    const Words<W> nd = load_other<W, CG>(p.other + (long long)yd * p.pitch + j0);
     Words<W> zu, zd;
     if constexpr (NDIM == 3) {
         const int pu = (z + 1 == p.lz ? 0 : z + 1) * p.ly + y;
         const int pd = (z == 0 ? p.lz - 1 : z - 1) * p.ly + y;
-        zu = load_words_ro<W>(p.other + (long long)pu * p.pitch + j0);
-        zd = load_words_ro<W>(p.other + (long long)pd * p.pitch + j0);
+        zu = load_other<W, CG>(p.other + (long long)pu * p.pitch + j0);
+        zd = load_other<W, CG>(p.other + (long long)pd * p.pitch + j0);
     }
     // horizontal neighbour byte outside this chunk's valid sites (periodic in x)
     const int je = par ? (j0 + 4 * wv == p.lh ? 0 : j0 + 4 * wv) : (j0 == 0 ? p.lh - 1 : j0 - 1);
-    const u32 edge = (u32)(uint8_t)__ldg(orow + je);
+    const u32 edge = CG ? (u32)(uint8_t)__ldcg(orow + je) : (u32)(uint8_t)__ldg(orow + je);
 
     Words<W> hz;
 #pragma unroll
@@ -232,6 +257,18 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
         m_acc += 2 * nv - 2 * (down + other_down);  // this colour's sites + the other's
         e_acc += 2 * anti - 2 * NDIM * nv;          // -(2d n - 2 anti)
     }
+}
+
+// A full chunk (all V sites valid) takes the guard-free instantiation; only a padded row's
+// last chunk pays for the valid-word checks.
+template <int V, int NDIM, int RULE, bool CG = false>
+__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
+                                           const u32* stab, long long& m_acc, long long& e_acc)
+{
+    if (j0 + V <= p.lh)
+        int8_chunk_impl<V, NDIM, RULE, CG, true>(p, row, y, z, j0, stab, m_acc, e_acc);
+    else
+        int8_chunk_impl<V, NDIM, RULE, CG, false>(p, row, y, z, j0, stab, m_acc, e_acc);
 }
 
 }  // namespace ising
