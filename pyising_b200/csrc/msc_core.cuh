@@ -113,7 +113,11 @@ __device__ __forceinline__ void msc_word(const MscHalf& p, int y, int x, long lo
 // The random numbers, bit levels and their order are the reference's; only the schedule
 // differs, so results are identical.  Lanes are handled as two independent 32-bit halves.
 
-constexpr int kQueueCap = 64;
+#ifndef ISING_MSC_POP
+#define ISING_MSC_POP 1
+#endif
+constexpr int kPop = 32 * ISING_MSC_POP;  // entries popped per pass (two per lane: two chains)
+constexpr int kQueueCap = kPop + 32;
 constexpr int kIntakeCalls = ISING_MSC_INTAKE_CALLS;  // Philox blocks per word before queueing
 
 struct QueueSlots {
@@ -199,7 +203,7 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
     bool more = next < end;
     if (more) intake_load(p, w, w < end, nw, nw_shift, L);
     while (true) {
-        if (n < 32 && more) {
+        if (n < kPop && more) {
             const bool valid = w < end;
             u32 a1l = 0, a1h = 0, undl = 0, undh = 0, resl = 0, resh = 0;
             if (valid) {
@@ -240,37 +244,53 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             n += __popc(km);
             __syncwarp();
         } else if (n > 0) {
-            const int take = n < 32 ? n : 32;
+            // pop up to kPop entries: lane l takes entries base + l and base + 32 + l
+            const int take = n < kPop ? n : kPop;
             const int base = n - take;
-            const bool act = lane < take;
-            u32 idx = 0, lp = 0;
-            u64 a1 = 0, und = 0, res = 0;
-            if (act) {
-                idx = q.idx[base + lane];
-                lp = q.lp[base + lane];
-                a1 = q.a1[base + lane];
-                und = q.und[base + lane];
-                res = q.res[base + lane];
+            u32 idx[ISING_MSC_POP], lp[ISING_MSC_POP];
+            u64 a1[ISING_MSC_POP];
+            u32 undl[ISING_MSC_POP], undh[ISING_MSC_POP], resl[ISING_MSC_POP], resh[ISING_MSC_POP];
+            bool act[ISING_MSC_POP];
+#pragma unroll
+            for (int m = 0; m < ISING_MSC_POP; ++m) {
+                const int e = base + 32 * m + lane;
+                act[m] = 32 * m + lane < take;
+                idx[m] = act[m] ? q.idx[e] : 0u;
+                lp[m] = act[m] ? q.lp[e] : 0u;
+                a1[m] = act[m] ? q.a1[e] : 0ull;
+                const u64 und = act[m] ? q.und[e] : 0ull, res = act[m] ? q.res[e] : 0ull;
+                undl[m] = (u32)und;
+                undh[m] = (u32)(und >> 32);
+                resl[m] = (u32)res;
+                resh[m] = (u32)(res >> 32);
             }
             __syncwarp();
-            u32 undl = (u32)und, undh = (u32)(und >> 32), resl = (u32)res, resh = (u32)(res >> 32);
-            if (act) {
-                const u32x4 r = philox4x32_10(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
-                call_levels(r, lvmask[lp], (u32)a1, (u32)(a1 >> 32), undl, undh, resl, resh);
-                ++lp;
+#pragma unroll
+            for (int m = 0; m < ISING_MSC_POP; ++m) {
+                if (act[m]) {
+                    const u32x4 r = philox4x32_10(idx[m], p.t, p.color, 1u + lp[m], p.k0, p.k1);
+                    call_levels(r, lvmask[lp[m]], (u32)a1[m], (u32)(a1[m] >> 32), undl[m],
+                                undh[m], resl[m], resh[m]);
+                    ++lp[m];
+                }
             }
-            const bool keep = act && (undl | undh) != 0 && lp < 16u;
-            if (act && !keep) p.own[idx] = (u64)resl | ((u64)resh << 32);
-            const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
-            if (keep) {
-                const int pos = base + __popc(km & lt);
-                q.idx[pos] = idx;
-                q.lp[pos] = lp;
-                q.a1[pos] = a1;
-                q.und[pos] = (u64)undl | ((u64)undh << 32);
-                q.res[pos] = (u64)resl | ((u64)resh << 32);
+            int kept = 0;
+#pragma unroll
+            for (int m = 0; m < ISING_MSC_POP; ++m) {
+                const bool keep = act[m] && (undl[m] | undh[m]) != 0 && lp[m] < 16u;
+                if (act[m] && !keep) p.own[idx[m]] = (u64)resl[m] | ((u64)resh[m] << 32);
+                const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
+                if (keep) {
+                    const int pos = base + kept + __popc(km & lt);
+                    q.idx[pos] = idx[m];
+                    q.lp[pos] = lp[m];
+                    q.a1[pos] = a1[m];
+                    q.und[pos] = (u64)undl[m] | ((u64)undh[m] << 32);
+                    q.res[pos] = (u64)resl[m] | ((u64)resh[m] << 32);
+                }
+                kept += __popc(km);
             }
-            n = base + __popc(km);
+            n = base + kept;
             __syncwarp();
         } else {
             break;
