@@ -56,7 +56,7 @@ struct BatchItem {
     long long begin, end;  // rows (int8) or words (msc)
 };
 
-template <int V, int NDIM, int RULE>
+template <int V, int NDIM, int RULE, bool MIXED>
 __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* __restrict__ lats,
                                                          const BatchItem* __restrict__ items,
                                                          int n_items, long long epoch)
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
                 y = (int)(row - (long long)z * L.ly);
             }
             for (int jc = tx; jc < p.cpr; jc += bx)
-                int8_chunk<V, NDIM, RULE>(p, row, y, z, jc * V, stab, m_acc, e_acc);
+                int8_chunk<V, NDIM, RULE, false, MIXED>(p, row, y, z, jc * V, stab, m_acc, e_acc);
         }
         if (meas) block_accumulate2(m_acc, e_acc, p.meas);
         __syncthreads();
@@ -182,10 +182,11 @@ struct Job {
 };
 
 struct KernelClass {
-    int variant, v, ndim, rule;
+    int variant, v, ndim, rule, mixed;  // mixed: rows padded (lh % 16 != 0)
     bool operator<(const KernelClass& o) const
     {
-        return std::tie(variant, v, ndim, rule) < std::tie(o.variant, o.v, o.ndim, o.rule);
+        return std::tie(variant, v, ndim, rule, mixed) <
+               std::tie(o.variant, o.v, o.ndim, o.rule, o.mixed);
     }
 };
 
@@ -487,7 +488,7 @@ private:
             L.k0 = (u32)s.seed;
             L.k1 = (u32)(s.seed >> 32);
             for (int i = 0; i < 7; ++i) L.table[i] = i < s.table_n ? s.table[i] : 0xFFFFFFFFu;
-            KernelClass kc{s.variant, 0, s.ndim, 0};
+            KernelClass kc{s.variant, 0, s.ndim, 0, 0};
             const int li = (int)lats.size();
             if (s.variant == ISING_VARIANT_MSC) {
                 const long long words = (long long)j.rows * j.nw;
@@ -502,6 +503,7 @@ private:
                 while (bx < L.cpr && bx < 128) bx <<= 1;
                 L.bx_log2 = __builtin_ctz((unsigned)bx);
                 kc.v = v;
+                kc.mixed = (j.lh % v) != 0;
                 kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
                 long long rpi = kInt8ItemSites / j.lh;
                 if (rpi < 1) rpi = 1;
@@ -552,13 +554,13 @@ private:
         return n_items < g ? n_items : g;
     }
 
-    template <int V, int NDIM>
+    template <int V, int NDIM, bool MIXED>
     cudaError_t launch_int8_rule(int rule, const BatchItem* it, int n)
     {
         switch (rule) {
 #define ISING_BATCH_CASE(R)                                                                   \
     case R: {                                                                                 \
-        auto fn = batch_int8_kernel<V, NDIM, R>;                                               \
+        auto fn = batch_int8_kernel<V, NDIM, R, MIXED>;                                        \
         fn<<<grid_for((const void*)fn, n), 256, 0, stream_>>>(d_lats_, it, n, epoch_);        \
         break;                                                                                \
     }
@@ -581,14 +583,13 @@ private:
                                                                                epoch_);
             return cudaGetLastError();
         }
-        if (kc.ndim == 3) {
-            if (kc.v == 16) return launch_int8_rule<16, 3>(kc.rule, it, n);
-            if (kc.v == 8) return launch_int8_rule<8, 3>(kc.rule, it, n);
-            return launch_int8_rule<4, 3>(kc.rule, it, n);
-        }
-        if (kc.v == 16) return launch_int8_rule<16, 2>(kc.rule, it, n);
-        if (kc.v == 8) return launch_int8_rule<8, 2>(kc.rule, it, n);
-        return launch_int8_rule<4, 2>(kc.rule, it, n);
+        // int8 rows are padded to 16 bytes, so the chunk width is always 16; lattices whose rows
+        // are a multiple of 16 get the kernel without the partial-chunk code.
+        if (kc.ndim == 3)
+            return kc.mixed ? launch_int8_rule<16, 3, true>(kc.rule, it, n)
+                            : launch_int8_rule<16, 3, false>(kc.rule, it, n);
+        return kc.mixed ? launch_int8_rule<16, 2, true>(kc.rule, it, n)
+                        : launch_int8_rule<16, 2, false>(kc.rule, it, n);
     }
 
     int retire()

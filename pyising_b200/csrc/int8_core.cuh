@@ -259,16 +259,21 @@ __device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row
     }
 }
 
-// A full chunk (all V sites valid) takes the guard-free instantiation; only a padded row's
+// MIXED = false: every chunk is full (lh % V == 0), only the guard-free code is compiled in.
+// MIXED = true: rows are padded; a full chunk still takes the guard-free code and only a row's
 // last chunk pays for the valid-word checks.
-template <int V, int NDIM, int RULE, bool CG = false>
+template <int V, int NDIM, int RULE, bool CG = false, bool MIXED = true>
 __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
                                            const u32* stab, long long& m_acc, long long& e_acc)
 {
-    if (j0 + V <= p.lh)
+    if constexpr (!MIXED) {
         int8_chunk_impl<V, NDIM, RULE, CG, true>(p, row, y, z, j0, stab, m_acc, e_acc);
-    else
-        int8_chunk_impl<V, NDIM, RULE, CG, false>(p, row, y, z, j0, stab, m_acc, e_acc);
+    } else {
+        if (j0 + V <= p.lh)
+            int8_chunk_impl<V, NDIM, RULE, CG, true>(p, row, y, z, j0, stab, m_acc, e_acc);
+        else
+            int8_chunk_impl<V, NDIM, RULE, CG, false>(p, row, y, z, j0, stab, m_acc, e_acc);
+    }
 }
 
 }  // namespace ising

@@ -4,7 +4,7 @@
 
 namespace ising {
 
-template <int V, int NDIM, int RULE>
+template <int V, int NDIM, int RULE, bool MIXED>
 __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
 {
     Int8Half p = p_in;
@@ -42,37 +42,37 @@ __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
             } else {
                 y = (int)row;
             }
-            int8_chunk<V, NDIM, RULE>(p, row, y, z, j0, stab, m_acc, e_acc);
+            int8_chunk<V, NDIM, RULE, false, MIXED>(p, row, y, z, j0, stab, m_acc, e_acc);
         }
     }
     if (p.meas) block_accumulate2(m_acc, e_acc, p.meas);
 }
 
 // ------------------------------------------------------------------------- host side ---
-template <int V, int NDIM>
+template <int V, int NDIM, bool MIXED>
 static cudaError_t launch_rule(int rule, const Int8Half& p, dim3 grid, dim3 block,
                                cudaStream_t st)
 {
     switch (rule) {
-    case kMetroFast: int8_half_kernel<V, NDIM, kMetroFast><<<grid, block, 0, st>>>(p); break;
-    case kHeatFast: int8_half_kernel<V, NDIM, kHeatFast><<<grid, block, 0, st>>>(p); break;
+    case kMetroFast: int8_half_kernel<V, NDIM, kMetroFast, MIXED><<<grid, block, 0, st>>>(p); break;
+    case kHeatFast: int8_half_kernel<V, NDIM, kHeatFast, MIXED><<<grid, block, 0, st>>>(p); break;
     case kMetroGeneric:
-        int8_half_kernel<V, NDIM, kMetroGeneric><<<grid, block, 0, st>>>(p);
+        int8_half_kernel<V, NDIM, kMetroGeneric, MIXED><<<grid, block, 0, st>>>(p);
         break;
     case kHeatGeneric:
-        int8_half_kernel<V, NDIM, kHeatGeneric><<<grid, block, 0, st>>>(p);
+        int8_half_kernel<V, NDIM, kHeatGeneric, MIXED><<<grid, block, 0, st>>>(p);
         break;
-    default: int8_half_kernel<V, NDIM, kObserve><<<grid, block, 0, st>>>(p); break;
+    default: int8_half_kernel<V, NDIM, kObserve, MIXED><<<grid, block, 0, st>>>(p); break;
     }
     return cudaGetLastError();
 }
 
-template <int V>
+template <int V, bool MIXED = false>
 static cudaError_t launch_v(int ndim, int rule, const Int8Half& p, dim3 grid, dim3 block,
                             cudaStream_t st)
 {
-    return ndim == 3 ? launch_rule<V, 3>(rule, p, grid, block, st)
-                     : launch_rule<V, 2>(rule, p, grid, block, st);
+    return ndim == 3 ? launch_rule<V, 3, MIXED>(rule, p, grid, block, st)
+                     : launch_rule<V, 2, MIXED>(rule, p, grid, block, st);
 }
 
 // Chunk width used for a row of lh bytes: the widest of 16/8/4 that divides it.
@@ -100,7 +100,10 @@ cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_bloc
     dim3 grid, block;
     int8_geometry(p.rows, p.cpr, max_blocks, &grid, &block);
     const int v = p.vw;
-    if (v == 16) return launch_v<16>(ndim, rule, p, grid, block, st);
+    if (v == 16) {  // padded rows (lh % 16 != 0) need the partial-chunk code
+        return (p.lh % 16) ? launch_v<16, true>(ndim, rule, p, grid, block, st)
+                           : launch_v<16, false>(ndim, rule, p, grid, block, st);
+    }
     if (v == 8) return launch_v<8>(ndim, rule, p, grid, block, st);
     return launch_v<4>(ndim, rule, p, grid, block, st);
 }
