@@ -39,37 +39,68 @@ struct BatchLattice {
     int rows, lh, ly, lz, cpr, nw, nw_shift;
     int pitch;             // int8: bytes between rows (lh rounded up to 16)
     u64 nw_magic;          // msc: ceil(2^64 / nw)
-    int bx_log2;           // int8: threads along a row = 1 << bx_log2 (of 256)
+    u32 cpr_magic;         // int8: fast_div magic of cpr (0: divide)
+    u32 ly_magic;          // int8 3D: fast_div magic of ly (0: divide)
     int every;             // measurement interval in sweeps (0 = none)
     u32 t0;
     u32 k0, k1;
     u32 table[7];
 };
 
-// Work-item sizes: ~64K int8 sites (whole rows) or 16K packed words (2K per warp).
-constexpr long long kInt8ItemSites = 65536;
-constexpr long long kMscItemWords = 16384;
+// Work-item sizes follow the work of each kernel class: about kItemsPerSlot items per resident
+// block of the class's kernel (so a launch has no long tail and small lattices still fill the
+// GPU), within these bounds; both are multiples of 256 chunks or words.
+constexpr long long kInt8ItemMin = 512, kInt8ItemMax = 4096;    // 16-byte chunks
+constexpr long long kMscItemMin = 2048, kMscItemMax = 16384;    // words
+constexpr long long kItemsPerSlot = 6;
+
+// Item size for `total` units of work over `slots` resident blocks.
+inline long long item_size(long long total, long long slots, long long lo, long long hi)
+{
+    long long want = (total + kItemsPerSlot * slots - 1) / (kItemsPerSlot * slots);
+    return want < lo ? lo : (want > hi ? hi : want);
+}
 
 struct BatchItem {
     int lat;
     int pad;
-    long long begin, end;  // rows (int8) or words (msc)
+    long long begin, end;  // chunks row * cpr + jc (int8) or words (msc)
 };
 
+// n / d for the divisors of one lattice: m = ceil(2^32 / d) when n * d < 2^32 holds for every n
+// the lattice can pass (then floor(n * m / 2^32) is exact), else m = 0 and a plain division.
+__device__ __forceinline__ u32 fast_div(u32 n, u32 d, u32 m) { return m ? __umulhi(n, m) : n / d; }
+
+inline u32 fast_div_magic(u32 d, unsigned long long n_max)
+{
+    if (d < 2 || n_max * d >= (1ull << 32)) return 0;
+    return (u32)(((1ull << 32) + d - 1) / d);
+}
+
+// One colour of every lattice of a kernel class.  A block walks its items grid-stride; an item
+// is a run of a lattice's chunks in row-major order (chunk c = row * cpr + jc), so all 256
+// threads have a chunk whatever the row length.
 template <int V, int NDIM, int RULE, bool MIXED>
 __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* __restrict__ lats,
                                                          const BatchItem* __restrict__ items,
                                                          int n_items, long long epoch)
 {
     __shared__ u32 stab[8];  // this item's acceptance table for the per-site lookup rules
+    constexpr bool kLookup = RULE != kMetroFast;
     const u32 color = (u32)(epoch & 1);
+    // (M, E) sums of the block's consecutive items of one lattice, added to the lattice's
+    // accumulators once, when the block's next item belongs to another lattice or it has none
+    // (one pair of same-address atomics per block and lattice instead of per item)
+    long long m_acc = 0, e_acc = 0;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const BatchLattice& L = lats[item.lat];
-        if (threadIdx.x < 7) stab[threadIdx.x] = L.table[threadIdx.x];
-        __syncthreads();
-        const long long s = (epoch - L.join_epoch) >> 1;
-        const bool meas = color == 1 && L.every > 0 && ((s + 1) % L.every) == 0;
+        if constexpr (kLookup) {
+            if (threadIdx.x < 7) stab[threadIdx.x] = L.table[threadIdx.x];
+            __syncthreads();
+        }
+        const u32 s = (u32)((epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
+        const bool meas = color == 1 && L.every > 0 && ((s + 1u) % (u32)L.every) == 0;
         Int8Half p;
         p.own = static_cast<int8_t*>(L.c[color]);
         p.other = static_cast<const int8_t*>(L.c[color ^ 1]);
@@ -80,30 +111,32 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
         p.cpr = L.cpr;
         p.pitch = L.pitch;
         p.vw = V;
-        p.t = L.t0 + (u32)s;
+        p.t = L.t0 + s;
         p.color = color;
         p.k0 = L.k0;
         p.k1 = L.k1;
 #pragma unroll
         for (int i = 0; i < 7; ++i) p.table[i] = L.table[i];
-        p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
+        p.meas = meas ? reinterpret_cast<unsigned long long*>(
+                            L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
                       : nullptr;
         p.ctl = nullptr;
-        const int bx = 1 << L.bx_log2;
-        const int tx = threadIdx.x & (bx - 1), ty = threadIdx.x >> L.bx_log2;
-        const int by = 256 >> L.bx_log2;
-        long long m_acc = 0, e_acc = 0;
-        for (long long row = item.begin + ty; row < item.end; row += by) {
+        const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, ly = (u32)L.ly, ly_m = L.ly_magic;
+        for (u32 c = (u32)item.begin + threadIdx.x; c < (u32)item.end; c += 256u) {
+            const u32 row = fast_div(c, cpr, cpr_m);
+            const int j0 = (int)(c - row * cpr) * V;
             int y = (int)row, z = 0;
             if constexpr (NDIM == 3) {
-                z = (int)(row / L.ly);
-                y = (int)(row - (long long)z * L.ly);
+                z = (int)fast_div(row, ly, ly_m);
+                y = (int)(row - (u32)z * ly);
             }
-            for (int jc = tx; jc < p.cpr; jc += bx)
-                int8_chunk<V, NDIM, RULE, false, MIXED>(p, row, y, z, jc * V, stab, m_acc, e_acc);
+            int8_chunk<V, NDIM, RULE, false, MIXED>(p, row, y, z, j0, stab, m_acc, e_acc);
         }
-        if (meas) block_accumulate2(m_acc, e_acc, p.meas);
-        __syncthreads();
+        if (meas && (it + (int)gridDim.x >= n_items || items[it + gridDim.x].lat != item.lat)) {
+            block_accumulate2(m_acc, e_acc, p.meas);
+            m_acc = e_acc = 0;
+        }
+        if constexpr (kLookup) __syncthreads();  // stab is rewritten by the next item
     }
 }
 
@@ -117,17 +150,18 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
     __shared__ uint4 lvmask[16];
     const u32 color = (u32)(epoch & 1);
     const int warp = threadIdx.x >> 5;
+    long long m_acc = 0, e_acc = 0;  // flushed per lattice, as in batch_int8_kernel
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const BatchLattice& L = lats[item.lat];
-        const long long s = (epoch - L.join_epoch) >> 1;
-        const bool meas = color == 1 && L.every > 0 && ((s + 1) % L.every) == 0;
+        const u32 s = (u32)((epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
+        const bool meas = color == 1 && L.every > 0 && ((s + 1u) % (u32)L.every) == 0;
         MscHalf p;
         p.own = static_cast<u64*>(L.c[color]);
         p.other = static_cast<const u64*>(L.c[color ^ 1]);
         p.rows = L.rows;
         p.nw = L.nw;
-        p.t = L.t0 + (u32)s;
+        p.t = L.t0 + s;
         p.color = color;
         p.k0 = L.k0;
         p.k1 = L.k1;
@@ -136,15 +170,19 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         p.nw_magic = L.nw_magic;
         p.stats = nullptr;
         p.ctl = nullptr;
-        p.meas = meas ? reinterpret_cast<unsigned long long*>(L.series + 2 * ((s + 1) / L.every - 1))
+        p.meas = meas ? reinterpret_cast<unsigned long long*>(
+                            L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
                       : nullptr;
         if (meas) {
-            long long m_acc = 0, e_acc = 0, ca = 0, wm = 0;
+            long long ca = 0, wm = 0;
             for (long long w = item.begin + threadIdx.x; w < item.end; w += blockDim.x) {
                 const int y = (int)(L.nw_shift >= 0 ? (w >> L.nw_shift) : div_magic(w, p.nw_magic, L.nw));
                 msc_word<true>(p, y, (int)(w - (long long)y * L.nw), m_acc, e_acc, ca, wm);
             }
-            block_accumulate2(m_acc, e_acc, p.meas);
+            if (it + (int)gridDim.x >= n_items || items[it + gridDim.x].lat != item.lat) {
+                block_accumulate2(m_acc, e_acc, p.meas);
+                m_acc = e_acc = 0;
+            }
         } else {
             if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
             __syncthreads();
@@ -201,6 +239,19 @@ public:
         e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
         sms_ = device_sm_count(device_);
+        // The engine's own stream-ordered pool keeps freed lattice memory (up to the budget)
+        // mapped across synchronisations, so admitting a job after another finished reuses it
+        // instead of mapping fresh pages; the device's default pool is left untouched.
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device_;
+        e = cudaMemPoolCreate(&pool_, &props);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolCreate");
+        uint64_t keep = (uint64_t)budget_;
+        e = cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolSetAttribute");
         return ISING_OK;
     }
 
@@ -208,11 +259,14 @@ public:
     {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
-        for (auto& kv : jobs_) free_job(*kv.second, true);
-        if (d_lats_) cudaFree(d_lats_);
-        if (d_items_) cudaFree(d_items_);
+        for (auto& kv : jobs_) free_job(*kv.second);
+        if (d_lats_) cudaFreeAsync(d_lats_, stream_);
+        if (d_items_) cudaFreeAsync(d_items_, stream_);
+        if (stream_) cudaStreamSynchronize(stream_);
+        for (auto& kv : pinned_free_) cudaFreeHost(kv.second);
         for (cudaEvent_t ev : epoch_events_) cudaEventDestroy(ev);
         if (stream_) cudaStreamDestroy(stream_);
+        if (pool_) cudaMemPoolDestroy(pool_);
         cudaGetLastError();
     }
 
@@ -339,7 +393,7 @@ public:
             return fail(ISING_ERR_STATE, "job %lld is still running", (long long)id);
         if (j.state == ISING_JOB_PENDING)
             pending_.erase(std::remove(pending_.begin(), pending_.end(), id), pending_.end());
-        free_job(j, false);
+        free_job(j);
         jobs_.erase(it);
         return ISING_OK;
     }
@@ -376,6 +430,8 @@ private:
         const int64_t ly = s.shape[s.ndim - 2], lz = s.ndim == 3 ? s.shape[0] : 1;
         if (ly * lz > 0x7FFFFFFF || lx / 2 > 0x7FFFFFFF)
             return fail(ISING_ERR_INVALID, "lattice too large");
+        if (s.variant == ISING_VARIANT_INT8 && ly * lz * ((lx / 2 + 15) / 16) > 0x7FFFFFFF)
+            return fail(ISING_ERR_INVALID, "lattice too large for the batch (2^31 chunks)");
         j.rows = (int)(ly * lz);
         j.lh = (int)(lx / 2);
         j.ly = (int)ly;
@@ -408,12 +464,12 @@ private:
     {
         cudaError_t e;
         for (int c = 0; c < 2; ++c) {
-            e = cudaMallocAsync(&j.c[c], j.colour_bytes, stream_);
+            e = dev_alloc(&j.c[c], j.colour_bytes);
             if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync (job lattice)");
         }
         if (j.series_pairs) {
             const size_t sb = j.series_pairs * 2 * sizeof(long long);
-            e = cudaMallocAsync((void**)&j.d_series, sb, stream_);
+            e = dev_alloc((void**)&j.d_series, sb);
             if (e == cudaSuccess) e = cudaMemsetAsync(j.d_series, 0, sb, stream_);
             if (e != cudaSuccess) return cuda_fail(e, "job series");
         }
@@ -430,7 +486,7 @@ private:
         } else {
             const size_t full = (size_t)j.rows * 2 * j.lh;
             int8_t* stage = nullptr;
-            e = cudaMallocAsync((void**)&stage, full, stream_);
+            e = dev_alloc((void**)&stage, full);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(stage, j.init.data(), full, cudaMemcpyHostToDevice, stream_);
             if (e == cudaSuccess) {
@@ -462,7 +518,8 @@ private:
     int rebuild()
     {
         std::vector<BatchLattice> lats;
-        std::map<KernelClass, std::vector<BatchItem>> by_class;
+        std::vector<KernelClass> lat_class;
+        std::map<KernelClass, long long> class_units;  // sites (int8) or words (msc) per class
         lats.reserve(active_.size());
         for (int64_t id : active_) {
             Job& j = *jobs_[id];
@@ -489,28 +546,41 @@ private:
             L.k1 = (u32)(s.seed >> 32);
             for (int i = 0; i < 7; ++i) L.table[i] = i < s.table_n ? s.table[i] : 0xFFFFFFFFu;
             KernelClass kc{s.variant, 0, s.ndim, 0, 0};
-            const int li = (int)lats.size();
             if (s.variant == ISING_VARIANT_MSC) {
-                const long long words = (long long)j.rows * j.nw;
-                for (long long b = 0; b < words; b += kMscItemWords)
-                    by_class[kc].push_back(
-                        BatchItem{li, 0, b, std::min(words, b + kMscItemWords)});
+                class_units[kc] += (long long)j.rows * j.nw;
             } else {
                 const int v = 16;  // rows padded to 16 bytes
                 L.pitch = j.pitch;
                 L.cpr = (j.lh + v - 1) / v;
-                int bx = 1;
-                while (bx < L.cpr && bx < 128) bx <<= 1;
-                L.bx_log2 = __builtin_ctz((unsigned)bx);
+                L.cpr_magic = fast_div_magic((u32)L.cpr, (unsigned long long)j.rows * L.cpr);
+                L.ly_magic = fast_div_magic((u32)j.ly, (unsigned long long)j.rows);
                 kc.v = v;
                 kc.mixed = (j.lh % v) != 0;
                 kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
-                long long rpi = kInt8ItemSites / j.lh;
-                if (rpi < 1) rpi = 1;
-                for (long long b = 0; b < j.rows; b += rpi)
-                    by_class[kc].push_back(BatchItem{li, 0, b, std::min<long long>(j.rows, b + rpi)});
+                class_units[kc] += (long long)j.rows * L.cpr;
             }
             lats.push_back(L);
+            lat_class.push_back(kc);
+        }
+        std::map<KernelClass, std::vector<BatchItem>> by_class;
+        for (int li = 0; li < (int)lats.size(); ++li) {
+            const BatchLattice& L = lats[li];
+            const KernelClass& kc = lat_class[li];
+            const long long units = class_units[kc];
+            std::vector<BatchItem>& out = by_class[kc];
+            if (L.variant == ISING_VARIANT_MSC) {
+                const long long words = (long long)L.rows * L.nw;
+                long long per = item_size(units, slots(kc), kMscItemMin, kMscItemMax);
+                per = (per + 255) / 256 * 256;
+                for (long long b = 0; b < words; b += per)
+                    out.push_back(BatchItem{li, 0, b, std::min(words, b + per)});
+            } else {
+                const long long chunks = (long long)L.rows * L.cpr;
+                long long per = item_size(units, slots(kc), kInt8ItemMin, kInt8ItemMax);
+                per = (per + 255) / 256 * 256;
+                for (long long b = 0; b < chunks; b += per)
+                    out.push_back(BatchItem{li, 0, b, std::min(chunks, b + per)});
+            }
         }
         std::vector<BatchItem> items;
         classes_.clear();
@@ -525,13 +595,23 @@ private:
         return rc;
     }
 
+    // Resident blocks of a class's kernel on the whole device.
+    long long slots(const KernelClass& kc)
+    {
+        const void* fn = kc.variant == ISING_VARIANT_MSC
+                             ? (const void*)batch_msc_kernel
+                             : (const void*)batch_int8_kernel<16, 2, kMetroFast, false>;
+        return (long long)sms_ * blocks_per_sm(fn, kc.variant == ISING_VARIANT_MSC
+                                                       ? kBatchWarps * 32 : 256);
+    }
+
     int upload(const void* src, size_t bytes, void** dst, size_t* cap)
     {
         if (bytes == 0) return ISING_OK;
         if (bytes > *cap) {
             if (*dst) cudaFreeAsync(*dst, stream_);
             size_t nc = std::max(bytes, *cap * 2);
-            cudaError_t e = cudaMallocAsync(dst, nc, stream_);
+            cudaError_t e = dev_alloc(dst, nc);
             if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync (work list)");
             *cap = nc;
         }
@@ -541,16 +621,21 @@ private:
         return ISING_OK;
     }
 
-    int grid_for(const void* fn, int n_items)
+    int blocks_per_sm(const void* fn, int threads)
     {
         int& per_sm = occupancy_[fn];
         if (per_sm < 1 &&
-            (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess ||
+            (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0) != cudaSuccess ||
              per_sm < 1)) {
             cudaGetLastError();
             per_sm = 2;
         }
-        const int g = sms_ * per_sm;
+        return per_sm;
+    }
+
+    int grid_for(const void* fn, int n_items, int threads = 256)
+    {
+        const int g = sms_ * blocks_per_sm(fn, threads);
         return n_items < g ? n_items : g;
     }
 
@@ -579,7 +664,7 @@ private:
         const BatchItem* it = d_items_ + off;
         if (kc.variant == ISING_VARIANT_MSC) {
             auto fn = batch_msc_kernel;
-            fn<<<grid_for((const void*)fn, n), kBatchWarps * 32, 0, stream_>>>(d_lats_, it, n,
+            fn<<<grid_for((const void*)fn, n, kBatchWarps * 32), kBatchWarps * 32, 0, stream_>>>(d_lats_, it, n,
                                                                                epoch_);
             return cudaGetLastError();
         }
@@ -614,15 +699,15 @@ private:
         cudaError_t e = cudaSuccess;
         if (j.series_pairs) {
             const size_t sb = j.series_pairs * 2 * sizeof(long long);
-            e = cudaMallocHost((void**)&j.h_series, sb);
+            e = pinned_get((void**)&j.h_series, sb);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(j.h_series, j.d_series, sb, cudaMemcpyDeviceToHost, stream_);
         }
         if (e == cudaSuccess && j.spec.keep_lattice) {
             const size_t full = (size_t)j.rows * 2 * j.lh;
             int8_t* stage = nullptr;
-            e = cudaMallocHost((void**)&j.h_lattice, full);
-            if (e == cudaSuccess) e = cudaMallocAsync((void**)&stage, full, stream_);
+            e = pinned_get((void**)&j.h_lattice, full);
+            if (e == cudaSuccess) e = dev_alloc((void**)&stage, full);
             if (e == cudaSuccess) {
                 if (j.spec.variant == ISING_VARIANT_MSC)
                     e = launch_msc_unpack((const u64*)j.c[0], (const u64*)j.c[1], stage, j.rows, 0,
@@ -698,26 +783,56 @@ public:
 
 private:
 
-    void free_job(Job& j, bool shutdown)
+    void free_job(Job& j)
     {
         if (j.done_event) cudaEventDestroy(j.done_event);
         j.done_event = nullptr;
         for (int c = 0; c < 2; ++c)
-            if (j.c[c]) (shutdown ? cudaFree(j.c[c]) : cudaFreeAsync(j.c[c], stream_));
-        if (j.d_series) (shutdown ? cudaFree(j.d_series) : cudaFreeAsync(j.d_series, stream_));
-        if (j.h_series) cudaFreeHost(j.h_series);
-        if (j.h_lattice) cudaFreeHost(j.h_lattice);
+            if (j.c[c]) cudaFreeAsync(j.c[c], stream_);
+        if (j.d_series) cudaFreeAsync(j.d_series, stream_);
+        if (j.h_series) pinned_put(j.h_series, j.series_pairs * 2 * sizeof(long long));
+        if (j.h_lattice) pinned_put(j.h_lattice, (size_t)j.rows * 2 * j.lh);
         j.c[0] = j.c[1] = nullptr;
         j.d_series = nullptr;
         j.h_series = nullptr;
         j.h_lattice = nullptr;
     }
 
+    cudaError_t dev_alloc(void** p, size_t bytes)
+    {
+        return cudaMallocFromPoolAsync(p, bytes, pool_, stream_);
+    }
+
+    // Pinned host buffers for results are reused across jobs (size classes of powers of two
+    // from 4 KiB): page-locking memory for every finished job would stall the serving loop.
+    static size_t pinned_class(size_t bytes)
+    {
+        size_t c = 4096;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+
+    cudaError_t pinned_get(void** p, size_t bytes)
+    {
+        const size_t c = pinned_class(bytes);
+        auto it = pinned_free_.find(c);
+        if (it != pinned_free_.end()) {
+            *p = it->second;
+            pinned_free_.erase(it);
+            return cudaSuccess;
+        }
+        return cudaMallocHost(p, c);
+    }
+
+    void pinned_put(void* p, size_t bytes) { pinned_free_.emplace(pinned_class(bytes), p); }
+
     int device_;
     int64_t budget_;
     int64_t used_ = 0;
     int sms_ = 148;
     cudaStream_t stream_ = nullptr;
+    cudaMemPool_t pool_ = nullptr;
+    std::multimap<size_t, void*> pinned_free_;  // reusable pinned result buffers by size class
     long long epoch_ = 0;
     int64_t last_id_ = 0;
     std::map<int64_t, std::unique_ptr<Job>> jobs_;

@@ -158,16 +158,24 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
 
 // Update (or, with RULE == kObserve, only measure) the V colour sites starting at j0 in row
 // `row` = (z, y) of the lattice in p; (M, E) contributions go to m_acc / e_acc when p.meas.
-template <int V, int NDIM, int RULE, bool CG = false, bool FULL = true>
-__device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row, int y, int z, int j0,
+//
+// MIXED = false: every chunk is full (lh % V == 0).  MIXED = true: rows are padded to a multiple
+// of V bytes and a row's last chunk holds wv < W valid words; such a chunk runs the same
+// instructions as a full one (no divergence inside a warp), with the padding words selected
+// away: their random numbers are drawn and discarded, their bytes stored back unchanged, and
+// the right-hand neighbour of the last valid word is the row's wrapped edge byte.
+template <int V, int NDIM, int RULE, bool CG = false, bool MIXED = true>
+__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
                                            const u32* stab, long long& m_acc, long long& e_acc)
 {
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
     const int par = (y + z + (int)p.color) & 1;
-    // Rows are `pitch` bytes apart; a row's last chunk may hold fewer than W valid words (the
-    // rest is padding, loaded but never updated, counted or used as a neighbour).
-    const int wv = FULL ? W : ((p.lh - j0 >= V) ? W : ((p.lh - j0) >> 2));
+    int wv = W;  // valid words of this chunk
+    if constexpr (MIXED) {
+        const int left = (p.lh - j0) >> 2;
+        wv = left < W ? left : W;
+    }
     const long long rb = row * p.pitch;
     const int8_t* orow = p.other + rb;
 
@@ -192,10 +200,11 @@ __device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row
 #pragma unroll
     for (int k = 0; k < W; ++k) {
         if (par) {
-            const u32 nx = (k + 1 < W && k + 1 < wv) ? c.v[(k + 1) % W] : edge;
+            u32 nx = edge;
+            if (k + 1 < W) nx = (!MIXED || k + 1 < wv) ? c.v[k + 1] : edge;
             hz.v[k] = __funnelshift_r(c.v[k], nx, 8);
         } else {
-            const u32 pv = (k > 0) ? c.v[(k + W - 1) % W] : (edge << 24);
+            const u32 pv = (k > 0) ? c.v[k - 1] : (edge << 24);
             hz.v[k] = __funnelshift_l(pv, c.v[k], 8);
         }
     }
@@ -218,7 +227,8 @@ __device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row
                 acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
             cnt[k] = acc >> 1;  // anti-aligned neighbours per site
         }
-        if (k < wv) other_down += __popc(c.v[k] & kBit1);
+        const int od = __popc(c.v[k] & kBit1);
+        other_down += (!MIXED || k < wv) ? od : 0;
     }
 
     Words<W> ns;
@@ -226,11 +236,12 @@ __device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row
     const u32 q0 = (u32)((unsigned long long)(row * p.lh + j0) >> 2);
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-        if (RULE == kObserve || k >= wv) {
+        if constexpr (RULE == kObserve) {
             ns.v[k] = s.v[k];
         } else {
             const u32x4 r = philox4x32_10(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
-            ns.v[k] = decide4<NDIM, RULE>(p, s.v[k], cnt[k], r, stab);
+            const u32 d = decide4<NDIM, RULE>(p, s.v[k], cnt[k], r, stab);
+            ns.v[k] = (!MIXED || k < wv) ? d : s.v[k];
         }
     }
     if constexpr (RULE != kObserve) store_words<W>(p.own + rb + j0, ns);
@@ -244,35 +255,18 @@ __device__ __forceinline__ void int8_chunk_impl(const Int8Half& p, long long row
         int anti = 0, down = 0;
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            if (k >= wv) continue;
             const u32 sv = ns.v[k];
             u32 sel;  // 0xFF in the bytes whose count is replaced by 2d - count
             if constexpr (kHeat) sel = ((sv & kBit1) >> 1) * 0xFFu;
             else sel = (((sv ^ s.v[k]) & kBit1) >> 1) * 0xFFu;
             const u32 ap = (cnt[k] & ~sel) | ((k2d - cnt[k]) & sel);
-            anti += byte_sum(ap);
-            down += __popc(sv & kBit1);
+            const bool valid = !MIXED || k < wv;
+            anti += valid ? byte_sum(ap) : 0;
+            down += valid ? __popc(sv & kBit1) : 0;
         }
         const int nv = 4 * wv;                      // valid sites of this chunk
         m_acc += 2 * nv - 2 * (down + other_down);  // this colour's sites + the other's
         e_acc += 2 * anti - 2 * NDIM * nv;          // -(2d n - 2 anti)
-    }
-}
-
-// MIXED = false: every chunk is full (lh % V == 0), only the guard-free code is compiled in.
-// MIXED = true: rows are padded; a full chunk still takes the guard-free code and only a row's
-// last chunk pays for the valid-word checks.
-template <int V, int NDIM, int RULE, bool CG = false, bool MIXED = true>
-__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
-                                           const u32* stab, long long& m_acc, long long& e_acc)
-{
-    if constexpr (!MIXED) {
-        int8_chunk_impl<V, NDIM, RULE, CG, true>(p, row, y, z, j0, stab, m_acc, e_acc);
-    } else {
-        if (j0 + V <= p.lh)
-            int8_chunk_impl<V, NDIM, RULE, CG, true>(p, row, y, z, j0, stab, m_acc, e_acc);
-        else
-            int8_chunk_impl<V, NDIM, RULE, CG, false>(p, row, y, z, j0, stab, m_acc, e_acc);
     }
 }
 
