@@ -67,14 +67,23 @@ struct BatchItem {
     long long begin, end;  // chunks row * cpr + jc (int8) or words (msc)
 };
 
-// n / d for the divisors of one lattice: m = ceil(2^32 / d) when n * d < 2^32 holds for every n
-// the lattice can pass (then floor(n * m / 2^32) is exact), else m = 0 and a plain division.
-__device__ __forceinline__ u32 fast_div(u32 n, u32 d, u32 m) { return m ? __umulhi(n, m) : n / d; }
-
-inline u32 fast_div_magic(u32 d, unsigned long long n_max)
+// The chunks [item.begin, item.end) of one lattice, 256 threads, row-major.
+template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
+__device__ __forceinline__ void batch_int8_item(const Int8Half& p, const BatchLattice& L,
+                                                const BatchItem& item, const u32* stab,
+                                                long long& m_acc, long long& e_acc)
 {
-    if (d < 2 || n_max * d >= (1ull << 32)) return 0;
-    return (u32)(((1ull << 32) + d - 1) / d);
+    const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, ly = (u32)L.ly, ly_m = L.ly_magic;
+    for (u32 c = (u32)item.begin + threadIdx.x; c < (u32)item.end; c += 256u) {
+        const u32 row = fast_div(c, cpr, cpr_m);
+        const int j0 = (int)(c - row * cpr) * V;
+        int y = (int)row, z = 0;
+        if constexpr (NDIM == 3) {
+            z = (int)fast_div(row, ly, ly_m);
+            y = (int)(row - (u32)z * ly);
+        }
+        int8_chunk<V, NDIM, RULE, false, MIXED, MEAS>(p, row, y, z, j0, stab, m_acc, e_acc);
+    }
 }
 
 // One colour of every lattice of a kernel class.  A block walks its items grid-stride; an item
@@ -121,17 +130,8 @@ __global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* 
                             L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
                       : nullptr;
         p.ctl = nullptr;
-        const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, ly = (u32)L.ly, ly_m = L.ly_magic;
-        for (u32 c = (u32)item.begin + threadIdx.x; c < (u32)item.end; c += 256u) {
-            const u32 row = fast_div(c, cpr, cpr_m);
-            const int j0 = (int)(c - row * cpr) * V;
-            int y = (int)row, z = 0;
-            if constexpr (NDIM == 3) {
-                z = (int)fast_div(row, ly, ly_m);
-                y = (int)(row - (u32)z * ly);
-            }
-            int8_chunk<V, NDIM, RULE, false, MIXED>(p, row, y, z, j0, stab, m_acc, e_acc);
-        }
+        if (meas) batch_int8_item<V, NDIM, RULE, MIXED, true>(p, L, item, stab, m_acc, e_acc);
+        else batch_int8_item<V, NDIM, RULE, MIXED, false>(p, L, item, stab, m_acc, e_acc);
         if (meas && (it + (int)gridDim.x >= n_items || items[it + gridDim.x].lat != item.lat)) {
             block_accumulate2(m_acc, e_acc, p.meas);
             m_acc = e_acc = 0;

@@ -735,6 +735,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.pitch = h->pitch;
         p.vw = h->vw;
         p.cpr = (h->lh + h->vw - 1) / h->vw;
+        p.band = h->band;
         p.t = t;
         p.color = (u32)color;
         p.k0 = k0;

@@ -21,6 +21,7 @@ struct ising_sim {
     int nw = 0;          // packed words per row (msc)
     int pitch = 0;       // int8: bytes between rows on the device (lh rounded up to 16)
     int vw = 16;         // int8: chunk width of the kernels
+    int band = 0;        // int8: rows per band of the band schedule (0: the launcher's default)
     uint64_t seed = 0;
     uint32_t table[7] = {0, 0, 0, 0, 0, 0, 0};
     int table_n = 5;
@@ -68,7 +69,8 @@ int selftest_bounded_wait(int device, int* timed_out);
 
 // kernel launchers
 int int8_chunk_width(int lh);
-void int8_geometry(long long rows, int cpr, int max_blocks, dim3* grid, dim3* block);
+int int8_default_band(long long rows, int ly, int cpr, int sm_count);
+unsigned int8_band_geometry(Int8Half& p, int max_blocks, int sm_count);
 cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_blocks,
                              cudaStream_t st);
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st);

@@ -112,6 +112,9 @@ struct Int8Half {
     int cpr;     // chunks per row = ceil(lh / V)
     int pitch;   // bytes between rows in memory (lh, or lh rounded up to 16 with V = 16)
     int vw;      // chunk width V: 16, 8 or 4 bytes
+    int band;    // band schedule: rows of one plane a thread walks (0: the launcher picks)
+    int bpp;     // band schedule: bands per plane = ceil(ly / band)
+    u32 cpr_magic, bpp_magic;  // fast_div magics of cpr and bpp (0: divide)
     u32 t;       // sweep counter (Philox counter word 1)
     u32 color;   // colour being updated (Philox counter word 2)
     u32 k0, k1;  // Philox key (seed lo, hi)
@@ -145,6 +148,17 @@ __device__ __forceinline__ long long div_magic(long long w, u64 m, int d)
 }
 
 inline u64 magic_for(int d) { return d > 1 ? ~0ull / (u64)d + 1ull : 0ull; }
+
+// n / d with m = ceil(2^32 / d) when n * d < 2^32 holds for every n passed (then
+// floor(n * m / 2^32) is exact: the error n * (m * d - 2^32) / (d * 2^32) stays below 1/d),
+// else m = 0 and a plain division.
+__device__ __forceinline__ u32 fast_div(u32 n, u32 d, u32 m) { return m ? __umulhi(n, m) : n / d; }
+
+inline u32 fast_div_magic(u32 d, unsigned long long n_max)
+{
+    if (d < 2 || n_max * d >= (1ull << 32)) return 0;
+    return (u32)(((1ull << 32) + d - 1) / d);
+}
 
 // Resolve the graph-replay control block of a launch (see Int8Half::ctl).
 template <typename P>

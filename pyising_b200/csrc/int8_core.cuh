@@ -156,46 +156,27 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
     }
 }
 
-// Update (or, with RULE == kObserve, only measure) the V colour sites starting at j0 in row
-// `row` = (z, y) of the lattice in p; (M, E) contributions go to m_acc / e_acc when p.meas.
+// New spins of the V colour sites starting at j0 in row `row` (parity `par` = (y + z + colour)
+// & 1) from their own words `s`, the opposite colour's words of the same row `c`, of the rows
+// above/below `nu`/`nd` and planes above/below `zu`/`zd` (3D), and the horizontal neighbour byte
+// outside the chunk `edge`; stores them, and with MEAS adds the chunk's (M, E) contribution to
+// m_acc / e_acc.  With RULE == kObserve nothing is updated (measurement only).
 //
 // MIXED = false: every chunk is full (lh % V == 0).  MIXED = true: rows are padded to a multiple
 // of V bytes and a row's last chunk holds wv < W valid words; such a chunk runs the same
 // instructions as a full one (no divergence inside a warp), with the padding words selected
 // away: their random numbers are drawn and discarded, their bytes stored back unchanged, and
 // the right-hand neighbour of the last valid word is the row's wrapped edge byte.
-template <int V, int NDIM, int RULE, bool CG = false, bool MIXED = true>
-__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
-                                           const u32* stab, long long& m_acc, long long& e_acc)
+template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
+__device__ __forceinline__ void int8_update(const Int8Half& p, long long row, int par, int j0,
+                                            int wv, const Words<V / 4>& s, const Words<V / 4>& c,
+                                            const Words<V / 4>& nu, const Words<V / 4>& nd,
+                                            const Words<V / 4>& zu, const Words<V / 4>& zd,
+                                            u32 edge, const u32* stab, long long& m_acc,
+                                            long long& e_acc)
 {
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
-    const int par = (y + z + (int)p.color) & 1;
-    int wv = W;  // valid words of this chunk
-    if constexpr (MIXED) {
-        const int left = (p.lh - j0) >> 2;
-        wv = left < W ? left : W;
-    }
-    const long long rb = row * p.pitch;
-    const int8_t* orow = p.other + rb;
-
-    const Words<W> s = load_words<W>(p.own + rb + j0);
-    const Words<W> c = load_other<W, CG>(orow + j0);
-    const int yu = z * p.ly + (y + 1 == p.ly ? 0 : y + 1);
-    const int yd = z * p.ly + (y == 0 ? p.ly - 1 : y - 1);
-    const Words<W> nu = load_other<W, CG>(p.other + (long long)yu * p.pitch + j0);
-    const Words<W> nd = load_other<W, CG>(p.other + (long long)yd * p.pitch + j0);
-    Words<W> zu, zd;
-    if constexpr (NDIM == 3) {
-        const int pu = (z + 1 == p.lz ? 0 : z + 1) * p.ly + y;
-        const int pd = (z == 0 ? p.lz - 1 : z - 1) * p.ly + y;
-        zu = load_other<W, CG>(p.other + (long long)pu * p.pitch + j0);
-        zd = load_other<W, CG>(p.other + (long long)pd * p.pitch + j0);
-    }
-    // horizontal neighbour byte outside this chunk's valid sites (periodic in x)
-    const int je = par ? (j0 + 4 * wv == p.lh ? 0 : j0 + 4 * wv) : (j0 == 0 ? p.lh - 1 : j0 - 1);
-    const u32 edge = CG ? (u32)(uint8_t)__ldcg(orow + je) : (u32)(uint8_t)__ldg(orow + je);
-
     Words<W> hz;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
@@ -227,8 +208,10 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
                 acc += ((zu.v[k] ^ sv) & kBit1) + ((zd.v[k] ^ sv) & kBit1);
             cnt[k] = acc >> 1;  // anti-aligned neighbours per site
         }
-        const int od = __popc(c.v[k] & kBit1);
-        other_down += (!MIXED || k < wv) ? od : 0;
+        if constexpr (MEAS) {
+            const int od = __popc(c.v[k] & kBit1);
+            other_down += (!MIXED || k < wv) ? od : 0;
+        }
     }
 
     Words<W> ns;
@@ -244,9 +227,9 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
             ns.v[k] = (!MIXED || k < wv) ? d : s.v[k];
         }
     }
-    if constexpr (RULE != kObserve) store_words<W>(p.own + rb + j0, ns);
+    if constexpr (RULE != kObserve) store_words<W>(p.own + row * p.pitch + j0, ns);
 
-    if (p.meas) {
+    if constexpr (MEAS) {
         // Bonds of this colour's sites: s*h = 2d - 2A' per site (A' = anti-aligned neighbours
         // of the new spin); E = -sum s*h.  A' follows from the counts: a flipped site's
         // anti-aligned neighbours are the previously aligned ones (2d - A), and for heat bath
@@ -267,6 +250,84 @@ __device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int
         const int nv = 4 * wv;                      // valid sites of this chunk
         m_acc += 2 * nv - 2 * (down + other_down);  // this colour's sites + the other's
         e_acc += 2 * anti - 2 * NDIM * nv;          // -(2d n - 2 anti)
+    }
+}
+
+template <bool MIXED, int W>
+__device__ __forceinline__ int valid_words(const Int8Half& p, int j0)
+{
+    if constexpr (!MIXED) return W;
+    const int left = (p.lh - j0) >> 2;
+    return left < W ? left : W;
+}
+
+// Horizontal neighbour byte outside a chunk's wv valid words (periodic in x).
+__device__ __forceinline__ int edge_index(const Int8Half& p, int par, int j0, int wv)
+{
+    return par ? (j0 + 4 * wv == p.lh ? 0 : j0 + 4 * wv) : (j0 == 0 ? p.lh - 1 : j0 - 1);
+}
+
+// One chunk (V sites from j0) of row `row` = (z, y): loads its neighbourhood, then int8_update.
+// CG reads the opposite colour from L2 (needed when one launch runs several half-sweeps).
+template <int V, int NDIM, int RULE, bool CG, bool MIXED, bool MEAS>
+__device__ __forceinline__ void int8_chunk(const Int8Half& p, long long row, int y, int z, int j0,
+                                           const u32* stab, long long& m_acc, long long& e_acc)
+{
+    constexpr int W = V / 4;
+    const int par = (y + z + (int)p.color) & 1;
+    const int wv = valid_words<MIXED, W>(p, j0);
+    const long long rb = row * p.pitch;
+    const int8_t* orow = p.other + rb;
+    const Words<W> s = load_words<W>(p.own + rb + j0);
+    const Words<W> c = load_other<W, CG>(orow + j0);
+    const int yu = z * p.ly + (y + 1 == p.ly ? 0 : y + 1);
+    const int yd = z * p.ly + (y == 0 ? p.ly - 1 : y - 1);
+    const Words<W> nu = load_other<W, CG>(p.other + (long long)yu * p.pitch + j0);
+    const Words<W> nd = load_other<W, CG>(p.other + (long long)yd * p.pitch + j0);
+    Words<W> zu = nu, zd = nd;
+    if constexpr (NDIM == 3) {
+        const int pu = (z + 1 == p.lz ? 0 : z + 1) * p.ly + y;
+        const int pd = (z == 0 ? p.lz - 1 : z - 1) * p.ly + y;
+        zu = load_other<W, CG>(p.other + (long long)pu * p.pitch + j0);
+        zd = load_other<W, CG>(p.other + (long long)pd * p.pitch + j0);
+    }
+    const int je = edge_index(p, par, j0, wv);
+    const u32 edge = CG ? (u32)(uint8_t)__ldcg(orow + je) : (u32)(uint8_t)__ldg(orow + je);
+    int8_update<V, NDIM, RULE, MIXED, MEAS>(p, row, par, j0, wv, s, c, nu, nd, zu, zd, edge, stab,
+                                            m_acc, e_acc);
+}
+
+// Band schedule: chunk column j0 of rows y0 .. y1-1 of plane z, top to bottom.  The three
+// opposite-colour rows a row needs (y-1, y, y+1) slide down the band, so each row loads one new
+// opposite-colour row (plus the planes z +- 1 in 3D) instead of three.
+template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
+__device__ __forceinline__ void int8_band(const Int8Half& p, int z, int y0, int y1, int j0,
+                                          const u32* stab, long long& m_acc, long long& e_acc)
+{
+    constexpr int W = V / 4;
+    const int wv = valid_words<MIXED, W>(p, j0);
+    const int ly = p.ly;
+    const long long plane = (long long)z * ly;
+    const int8_t* oth = p.other + j0;
+    Words<W> nd = load_words_ro<W>(oth + (plane + (y0 == 0 ? ly - 1 : y0 - 1)) * p.pitch);
+    Words<W> c = load_words_ro<W>(oth + (plane + y0) * p.pitch);
+    const long long zup = NDIM == 3 ? (long long)(z + 1 == p.lz ? 0 : z + 1) * ly : 0;
+    const long long zdn = NDIM == 3 ? (long long)(z == 0 ? p.lz - 1 : z - 1) * ly : 0;
+    for (int y = y0; y < y1; ++y) {
+        const long long row = plane + y;
+        const Words<W> nu = load_words_ro<W>(oth + (plane + (y + 1 == ly ? 0 : y + 1)) * p.pitch);
+        Words<W> zu = nu, zd = nd;
+        if constexpr (NDIM == 3) {
+            zu = load_words_ro<W>(oth + (zup + y) * p.pitch);
+            zd = load_words_ro<W>(oth + (zdn + y) * p.pitch);
+        }
+        const int par = (y + z + (int)p.color) & 1;
+        const u32 edge = (u32)(uint8_t)__ldg(p.other + row * p.pitch + edge_index(p, par, j0, wv));
+        const Words<W> s = load_words<W>(p.own + row * p.pitch + j0);
+        int8_update<V, NDIM, RULE, MIXED, MEAS>(p, row, par, j0, wv, s, c, nu, nd, zu, zd, edge,
+                                                stab, m_acc, e_acc);
+        nd = c;
+        c = nu;
     }
 }
 

@@ -111,8 +111,14 @@ __global__ void __launch_bounds__(256) int8_persistent_kernel(const PersistArgs 
         long long m_acc = 0, e_acc = 0;
         if (b == a.mute_band) break;  // test hook: this band never publishes (neighbours time out)
         for (long long row = r0 + ty; row < r1; row += by)
-            for (int jc = tx; jc < p.cpr; jc += bx)
-                int8_chunk<16, 2, RULE, true>(p, row, (int)row, 0, jc * 16, stab, m_acc, e_acc);
+            for (int jc = tx; jc < p.cpr; jc += bx) {
+                if (meas)
+                    int8_chunk<16, 2, RULE, true, true, true>(p, row, (int)row, 0, jc * 16, stab,
+                                                              m_acc, e_acc);
+                else
+                    int8_chunk<16, 2, RULE, true, true, false>(p, row, (int)row, 0, jc * 16, stab,
+                                                               m_acc, e_acc);
+            }
         if (meas) block_accumulate2(m_acc, e_acc, p.meas);
         __syncthreads();  // every row of the band is written (CTA scope) ...
         if (threadIdx.x == 0) {

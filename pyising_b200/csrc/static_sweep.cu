@@ -12,6 +12,7 @@
 // its 64 KiB until the process exits.  Host code cannot use the symbol's name as an address
 // (on the host it names a host-side stand-in), so each device's real address is looked up once
 // with cudaGetSymbolAddress, with that device current, and cached.
+#include <cstring>
 #include <mutex>
 
 #include "capi_internal.h"
@@ -152,6 +153,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 e = launch_msc_half(true, p, max_blocks, st);
             } else {
                 Int8Half p;
+                memset(&p, 0, sizeof p);
                 p.own = static_cast<int8_t*>(own);
                 p.other = static_cast<const int8_t*>(other);
                 p.rows = rows;
