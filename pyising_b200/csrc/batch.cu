@@ -39,8 +39,9 @@ struct BatchLattice {
     int rows, lh, ly, lz, cpr, nw, nw_shift;
     int pitch;             // int8: bytes between rows (lh rounded up to 16)
     u64 nw_magic;          // msc: ceil(2^64 / nw)
+    int band, bpp;         // int8: rows per band and bands per plane (band schedule)
     u32 cpr_magic;         // int8: fast_div magic of cpr (0: divide)
-    u32 ly_magic;          // int8 3D: fast_div magic of ly (0: divide)
+    u32 bpp_magic;         // int8 3D: fast_div magic of bpp (0: divide)
     int every;             // measurement interval in sweeps (0 = none)
     u32 t0;
     u32 k0, k1;
@@ -50,7 +51,7 @@ struct BatchLattice {
 // Work-item sizes follow the work of each kernel class: about kItemsPerSlot items per resident
 // block of the class's kernel (so a launch has no long tail and small lattices still fill the
 // GPU), within these bounds; both are multiples of 256 chunks or words.
-constexpr long long kInt8ItemMin = 512, kInt8ItemMax = 4096;    // 16-byte chunks
+constexpr long long kInt8ItemMin = 512, kInt8ItemMax = 4096;    // band slots
 constexpr long long kMscItemMin = 2048, kMscItemMax = 16384;    // words
 constexpr long long kItemsPerSlot = 6;
 
@@ -64,33 +65,42 @@ inline long long item_size(long long total, long long slots, long long lo, long 
 struct BatchItem {
     int lat;
     int pad;
-    long long begin, end;  // chunks row * cpr + jc (int8) or words (msc)
+    long long begin, end;  // band slots band * cpr + jc (int8) or words (msc)
 };
 
-// The chunks [item.begin, item.end) of one lattice, 256 threads, row-major.
+// The slots [item.begin, item.end) of one lattice, 256 threads: slot = band * cpr + jc, a band
+// being L.band rows of one plane that the thread walks top to bottom (int8_band).
 template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
 __device__ __forceinline__ void batch_int8_item(const Int8Half& p, const BatchLattice& L,
                                                 const BatchItem& item, const u32* stab,
                                                 long long& m_acc, long long& e_acc)
 {
-    const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, ly = (u32)L.ly, ly_m = L.ly_magic;
-    for (u32 c = (u32)item.begin + threadIdx.x; c < (u32)item.end; c += 256u) {
-        const u32 row = fast_div(c, cpr, cpr_m);
-        const int j0 = (int)(c - row * cpr) * V;
-        int y = (int)row, z = 0;
+    const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, bpp = (u32)L.bpp, bpp_m = L.bpp_magic;
+    for (u32 slot = (u32)item.begin + threadIdx.x; slot < (u32)item.end; slot += 256u) {
+        const u32 band = fast_div(slot, cpr, cpr_m);
+        const int j0 = (int)(slot - band * cpr) * V;
+        int z = 0, yb = (int)band;
         if constexpr (NDIM == 3) {
-            z = (int)fast_div(row, ly, ly_m);
-            y = (int)(row - (u32)z * ly);
+            z = (int)fast_div(band, bpp, bpp_m);
+            yb = (int)(band - (u32)z * bpp);
         }
-        int8_chunk<V, NDIM, RULE, false, MIXED, MEAS>(p, row, y, z, j0, stab, m_acc, e_acc);
+        const int y0 = yb * L.band;
+        const int y1 = y0 + L.band < L.ly ? y0 + L.band : L.ly;
+        int8_band<V, NDIM, RULE, MIXED, MEAS>(p, z, y0, y1, j0, stab, m_acc, e_acc);
     }
 }
 
 // One colour of every lattice of a kernel class.  A block walks its items grid-stride; an item
-// is a run of a lattice's chunks in row-major order (chunk c = row * cpr + jc), so all 256
-// threads have a chunk whatever the row length.
+// is a run of a lattice's band slots (band-major), so all 256 threads have a slot whatever the
+// row length.
 template <int V, int NDIM, int RULE, bool MIXED>
-__global__ void __launch_bounds__(256, 3) batch_int8_kernel(const BatchLattice* __restrict__ lats,
+// Two resident blocks per SM (up to 128 registers): the lattice parameters of an item live in
+// registers here (they are kernel parameters in the single-lattice kernel), and three blocks
+// per SM (80 registers) spilled and measured slower.
+#ifndef ISING_BATCH_MIN_BLOCKS
+#define ISING_BATCH_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, ISING_BATCH_MIN_BLOCKS) batch_int8_kernel(const BatchLattice* __restrict__ lats,
                                                          const BatchItem* __restrict__ items,
                                                          int n_items, long long epoch)
 {
@@ -173,25 +183,22 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         p.meas = meas ? reinterpret_cast<unsigned long long*>(
                             L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
                       : nullptr;
+        if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+        __syncthreads();
+        const long long len = item.end - item.begin;
+        long long per = (len + kBatchWarps - 1) / kBatchWarps;
+        per = (per + 31) / 32 * 32;
+        const long long b = item.begin + warp * per;
+        const long long e = min(b + per, item.end);
+        msc_queue_range(p, b, e, L.nw_shift, q_all[warp], lvmask);
         if (meas) {
-            long long ca = 0, wm = 0;
-            for (long long w = item.begin + threadIdx.x; w < item.end; w += blockDim.x) {
-                const int y = (int)(L.nw_shift >= 0 ? (w >> L.nw_shift) : div_magic(w, p.nw_magic, L.nw));
-                msc_word<true>(p, y, (int)(w - (long long)y * L.nw), m_acc, e_acc, ca, wm);
-            }
+            // the warp's words are final: measure them (the other colour is unchanged)
+            __syncwarp();
+            msc_measure_range(p, b, e, L.nw_shift, m_acc, e_acc);
             if (it + (int)gridDim.x >= n_items || items[it + gridDim.x].lat != item.lat) {
                 block_accumulate2(m_acc, e_acc, p.meas);
                 m_acc = e_acc = 0;
             }
-        } else {
-            if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
-            __syncthreads();
-            const long long len = item.end - item.begin;
-            long long per = (len + kBatchWarps - 1) / kBatchWarps;
-            per = (per + 31) / 32 * 32;
-            const long long b = item.begin + warp * per;
-            const long long e = min(b + per, item.end);
-            msc_queue_range(p, b, e, L.nw_shift, q_all[warp], lvmask);
         }
         __syncthreads();
     }
@@ -552,8 +559,7 @@ private:
                 const int v = 16;  // rows padded to 16 bytes
                 L.pitch = j.pitch;
                 L.cpr = (j.lh + v - 1) / v;
-                L.cpr_magic = fast_div_magic((u32)L.cpr, (unsigned long long)j.rows * L.cpr);
-                L.ly_magic = fast_div_magic((u32)j.ly, (unsigned long long)j.rows);
+
                 kc.v = v;
                 kc.mixed = (j.lh % v) != 0;
                 kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
@@ -563,6 +569,7 @@ private:
             lat_class.push_back(kc);
         }
         std::map<KernelClass, std::vector<BatchItem>> by_class;
+        std::map<KernelClass, int> class_band;
         for (int li = 0; li < (int)lats.size(); ++li) {
             const BatchLattice& L = lats[li];
             const KernelClass& kc = lat_class[li];
@@ -575,11 +582,24 @@ private:
                 for (long long b = 0; b < words; b += per)
                     out.push_back(BatchItem{li, 0, b, std::min(words, b + per)});
             } else {
-                const long long chunks = (long long)L.rows * L.cpr;
-                long long per = item_size(units, slots(kc), kInt8ItemMin, kInt8ItemMax);
+                // the class's band height: the longest of 8, 4, 2, 1 rows that still leaves
+                // kItemsPerSlot items of one slot per thread for every resident block
+                int& band = class_band[kc];
+                if (band == 0) {
+                    const long long want = kItemsPerSlot * 256 * slots(kc);
+                    band = 8;
+                    while (band > 1 && units / band < want) band >>= 1;
+                }
+                BatchLattice& M = lats[li];
+                M.band = band < M.ly ? band : M.ly;
+                M.bpp = (M.ly + M.band - 1) / M.band;
+                const long long nslots = (long long)M.lz * M.bpp * M.cpr;
+                M.cpr_magic = fast_div_magic((u32)M.cpr, (unsigned long long)nslots);
+                M.bpp_magic = fast_div_magic((u32)M.bpp, (unsigned long long)M.lz * M.bpp);
+                long long per = item_size(units / M.band, slots(kc), kInt8ItemMin, kInt8ItemMax);
                 per = (per + 255) / 256 * 256;
-                for (long long b = 0; b < chunks; b += per)
-                    out.push_back(BatchItem{li, 0, b, std::min(chunks, b + per)});
+                for (long long b = 0; b < nslots; b += per)
+                    out.push_back(BatchItem{li, 0, b, std::min(nslots, b + per)});
             }
         }
         std::vector<BatchItem> items;

@@ -298,4 +298,17 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
     }
 }
 
+// (M, E) contributions of words [begin, end) as they are now, one word per lane of the warp:
+// run after the warp's msc_queue_range (and a __syncwarp) to measure the updated colour.
+__device__ __forceinline__ void msc_measure_range(const MscHalf& p, long long begin, long long end,
+                                                  int nw_shift, long long& m_acc,
+                                                  long long& e_acc)
+{
+    long long calls = 0, wmax = 0;
+    for (long long w = begin + (threadIdx.x & 31); w < end; w += 32) {
+        const int y = (int)(nw_shift >= 0 ? (w >> nw_shift) : div_magic(w, p.nw_magic, p.nw));
+        msc_word<false>(p, y, (int)(w - (long long)y * p.nw), m_acc, e_acc, calls, wmax);
+    }
+}
+
 }  // namespace ising

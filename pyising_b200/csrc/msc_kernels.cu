@@ -1,6 +1,7 @@
-// Single-lattice multi-spin-coded half-sweep kernels: the one-word-per-thread kernel (used for
-// measured sweeps, the observables reduction and the call statistics) and the work-stack kernel
-// (every other sweep).  Device code in msc_core.cuh.
+// Single-lattice multi-spin-coded half-sweep kernels: the work-stack kernel (every sweep; a
+// measured half-sweep measures each warp's words after updating them) and the one-word-per-
+// thread kernel (the observables reduction and the call statistics).  Device code in
+// msc_core.cuh.
 #include "msc_core.cuh"
 
 #ifndef ISING_MSC_MIN_BLOCKS
@@ -40,6 +41,13 @@ __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
     const long long begin = ((long long)blockIdx.x * kQueueWarps + (threadIdx.x >> 5)) * per_warp;
     const long long end = min(begin + per_warp, total);
     msc_queue_range(p, begin, end, nw_shift, q_all[threadIdx.x >> 5], lvmask);
+    if (p.meas) {
+        // the warp's words are final: measure them (the other colour is unchanged)
+        __syncwarp();
+        long long m_acc = 0, e_acc = 0;
+        msc_measure_range(p, begin, end, nw_shift, m_acc, e_acc);
+        block_accumulate2(m_acc, e_acc, p.meas);
+    }
 }
 
 void msc_geometry(int rows, int nw, int max_blocks, dim3* grid, dim3* block)
@@ -81,7 +89,7 @@ int msc_nw_shift(int nw) { return (nw & (nw - 1)) == 0 ? __builtin_ctz((unsigned
 
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st)
 {
-    if (update && !p.meas && !p.stats) {
+    if (update && !p.stats) {
         // one resident wave of warps, each with an equal contiguous range of words
         const long long total = (long long)p.rows * p.nw;
         const int sms = max_blocks / 8 > 0 ? max_blocks / 8 : 1;
