@@ -155,14 +155,30 @@ def make_sim(wl: str, seed_offset: int = 0):
     return cls(shape, beta, seed=seed + seed_offset, algorithm=alg, init=init)
 
 
+def tune_workload(wl: str, device: int) -> dict:
+    """The autotuner's launch knobs for a workload's shape (measured on a scratch lattice before
+    any timing; not written to the user's tuning cache)."""
+    from pyising_b200 import autotune
+
+    variant, shape, alg, beta, *_ = WORKLOADS[wl]
+    res = autotune.tune(variant, shape, alg, beta, device=device, save=False)
+    return {"config": res["config"], "default_flips_per_ns": round(res["default_flips_per_ns"], 1),
+            "tuned_flips_per_ns": round(res["flips_per_ns"], 1),
+            "seconds": round(res["seconds"], 2)}
+
+
 def run_device(wl: str, steps: int, warmup: int, rank: int, world: int, local: int,
-               dist) -> dict:
+               dist, tuned: dict | None = None) -> dict:
     """Device-resident timing: K steps, CUDA events on the launching stream, L2 flushed."""
     import torch
+
+    from pyising_b200 import autotune
 
     variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
     every = MEASURE_EVERY.get(wl, 0)
     sim = make_sim(wl, rank)
+    if tuned:
+        autotune.apply(sim, tuned["config"])
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
     st0 = sim.state()
@@ -205,25 +221,40 @@ def run_device(wl: str, steps: int, warmup: int, rank: int, world: int, local: i
     n = int(np.prod(shape))
     flips = n * sweeps * steps * world
     value = flips / (total_ms * 1e6)
-    launches = 2 * sweeps * steps
+    launches = 2 * sweeps * steps  # half-sweeps: the unit of the roofline's launch time
     avg_launch_ms = total_ms / launches
+    # kernels launched in the timed region: every half-sweep, plus one counter node per
+    # replayed graph chunk and one counter reset per call; a persistent run is one launch
+    cfg = (tuned or {}).get("config", {})
+    if cfg.get("schedule") == "persistent" and variant == "int8" and len(shape) == 2:
+        per_step = 1
+    elif cfg.get("schedule") == "launches":
+        per_step = 2 * sweeps
+    else:
+        g = every if every else int(cfg.get("graph_chunk", 32))
+        per_step = 2 * sweeps + (sweeps // g + 1 if sweeps >= 2 * g else 0)
     M, E = sim.observables_int()
     out = {"value": value, "ms_per_step": total_ms / steps, "step_ms": ms,
-           "launches": launches, "avg_launch_ms": avg_launch_ms, "flips_per_step": n * sweeps,
+           "launches": launches, "gpu_launches": per_step * steps,
+           "avg_launch_ms": avg_launch_ms, "flips_per_step": n * sweeps,
            "final_M": M, "final_E": E, "clocks": clk.summary(), "n_spins": n,
            "bytes_per_update": bpu, "sim": sim}
     del flush
     return out
 
 
-def run_e2e(wl: str, steps: int, rank: int, world: int, dist) -> dict:
+def run_e2e(wl: str, steps: int, rank: int, world: int, dist, tuned: dict | None = None) -> dict:
     """The same job through the public API with host buffers: upload the start configuration,
     sweep, download the final colour arrays and read (M, E), every step."""
     import torch
 
+    from pyising_b200 import autotune
+
     variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
     every = MEASURE_EVERY.get(wl, 0)
     sim = make_sim(wl, rank)
+    if tuned:
+        autotune.apply(sim, tuned["config"])
     st0 = sim.state()
     c0, c1 = st0["c0"], st0["c1"]
     h2d = c0.nbytes + c1.nbytes + sim.table.nbytes
@@ -363,11 +394,15 @@ def run_batched_ensemble() -> dict:
     """C4: batched vs one at a time, every lattice's series compared."""
     import torch
 
+    from pyising_b200 import autotune
     from pyising_b200.ensemble import Ensemble
 
     jobs = c4_jobs()
     flips = sum(j.n_spins * j.sweeps for j in jobs)
+    tuned = autotune.tune_ensemble(jobs, sweeps=100)
     with Ensemble(memory_budget=120e9) as ens:
+        for name, v in tuned["config"].items():
+            ens.set_knob(name, v)
         ids = [ens.add(j) for j in jobs]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -383,6 +418,7 @@ def run_batched_ensemble() -> dict:
             "batched_flips_per_ns": round(flips / t_batch / 1e9, 2),
             "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
             "speedup": round(t_seq / t_batch, 3), "bit_identical": bool(same),
+            "tuned_batch_knobs": tuned["config"],
             "timed": "uploads of the start lattices, all sweeps, series back to the host"}
 
 
@@ -392,11 +428,16 @@ def run_served_stream(n_jobs: int) -> dict:
 
     from pyising_b200.ensemble import Server
 
+    from pyising_b200 import autotune
+
     arrivals, jobs = c5_jobs(n_jobs)
     flips = sum(j.n_spins * j.sweeps for j in jobs)
     submit_t = [0.0] * n_jobs
     ids = [0] * n_jobs
+    tuned = autotune.tune_ensemble(jobs[: min(n_jobs, 100)], sweeps=100)
     with Server(memory_budget=120e9) as srv:
+        for name, v in tuned["config"].items():
+            srv.set_knob(name, v)
         start = time.perf_counter()
 
         def feeder():
@@ -432,7 +473,8 @@ def run_served_stream(n_jobs: int) -> dict:
             "speedup": round(t_seq / served_s, 3),
             "latency_p50_s": round(float(np.percentile(lat, 50)), 4),
             "latency_p99_s": round(float(np.percentile(lat, 99)), 4),
-            "bit_identical": bool(same), "memory_budget_bytes": int(120e9)}
+            "bit_identical": bool(same), "memory_budget_bytes": int(120e9),
+            "tuned_batch_knobs": tuned["config"]}
 
 
 def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
@@ -440,9 +482,10 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
 
     wl = args.workload
     variant, shape, alg, beta, init, seed, sweeps, bpu = WORKLOADS[wl]
-    dev = run_device(wl, args.steps, args.warmup, rank, world, local, dist)
+    tuned = tune_workload(wl, local) if args.tune else None
+    dev = run_device(wl, args.steps, args.warmup, rank, world, local, dist, tuned)
     sim = dev.pop("sim")
-    e2e = run_e2e(wl, max(1, min(args.steps, 3)), rank, world, dist)
+    e2e = run_e2e(wl, max(1, min(args.steps, 3)), rank, world, dist, tuned)
     if rank != 0:
         return None
     peaks = measured_peaks()
@@ -462,7 +505,8 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
                    "algorithm": alg, "beta": beta, "sweeps_per_step": sweeps,
                    "l2": "flushed between steps (256 MiB write); the lattice stays "
                          "L2-resident within a step",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "launch_knobs": tuned if tuned else "library defaults"},
         "pct_hbm_roofline": round(100 * dev["value"] / hbm_ceiling, 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -474,7 +518,7 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
                      "avg_launch_ms": round(dev["avg_launch_ms"], 5)},
         "rng_roofline": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in rng.items()},
         "e2e": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in e2e.items()},
-        "gpu_launches": dev["launches"],
+        "gpu_launches": dev["gpu_launches"],
         "clocks": dev["clocks"],
         "final_M_E": [dev["final_M"], dev["final_E"]],
     }
@@ -486,13 +530,15 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
         for other in WORKLOADS:
             if other == wl:
                 continue
-            d = run_device(other, 3, 3, 0, 1, local, None)
+            t_other = tune_workload(other, local) if args.tune else None
+            d = run_device(other, 3, 3, 0, 1, local, None, t_other)
             d.pop("sim")
             v, _, _, _, _, _, sw, b = WORKLOADS[other]
             extras[other] = {"flips_per_ns": round(d["value"], 2),
                              "ms_per_step": round(d["ms_per_step"], 4),
                              "pct_hbm_roofline": round(100 * d["value"] * b / peaks["hbm_gbs"], 2),
-                             "description": DESCRIPTION[other]}
+                             "description": DESCRIPTION[other],
+                             "launch_knobs": t_other if t_other else "library defaults"}
         line["other_configs"] = extras
     if args.batch and world == 1:
         line["batched_ensemble"] = run_batched_ensemble()
@@ -550,6 +596,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="msc16384")
     ap.add_argument("--no-extras", dest="extras", action="store_false")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="time the library's default launch knobs instead of tuned ones")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 96-lattice batched ensemble")
     ap.add_argument("--serve-jobs", type=int, default=300,

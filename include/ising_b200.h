@@ -48,6 +48,10 @@ int ising_version(void);
  * Replaces: pyising.backends._gpu.cuda_available (src/pyising/backends/_gpu.py:39-45). */
 int ising_device_count(int* n);
 
+/* "<name> sm_<major><minor> <n> SMs" of a device (the autotuner's cache key).  No counterpart
+ * in the reference. */
+int ising_device_name(int device, char* buf, int buflen);
+
 /* Create a simulation: ndim 2 or 3; shape is (Ly, Lx) or (Lz, Ly, Lx); every extent even and
  * >= 2; Lx % 8 == 0 (int8) or Lx % 128 == 0 (msc, 2D Metropolis only).  Device arrays are
  * allocated but not initialised: call ising_set_lattice / ising_upload / ising_fill_cold.
@@ -119,6 +123,34 @@ int ising_half_sweep(ising_sim* h, int color, uint64_t t);
 #define ISING_SCHEDULE_GRAPHS 2
 #define ISING_SCHEDULE_PERSISTENT 3
 int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
+
+/* Launch knobs of a handle, picked by the autotuner (pyising_b200.autotune) or by hand.  Every
+ * value gives identical spins and observables; only the speed changes.  Setting a knob drops
+ * the handle's captured graphs.  No counterpart in the reference, whose kernels have a fixed
+ * launch shape (src/pyising/backends/cupy_backend.py:68-72,129-135).
+ *   ISING_KNOB_BAND           int8: rows of one plane a thread walks, reusing the opposite
+ *                             colour's rows (halo depth); 0 = occupancy-based default
+ *   ISING_KNOB_CHUNK_WIDTH    int8: bytes (4 sites each per 32-bit word) per thread: 16, 8, 4
+ *   ISING_KNOB_BLOCKS_PER_SM  grid cap in blocks of 256 threads per SM (default 8)
+ *   ISING_KNOB_MSC_WAVES      msc: warp ranges per resident warp (default 1)
+ *   ISING_KNOB_GRAPH_CHUNK    sweeps per captured graph of an unmeasured run (default 32) */
+#define ISING_KNOB_BAND 1
+#define ISING_KNOB_CHUNK_WIDTH 2
+#define ISING_KNOB_BLOCKS_PER_SM 3
+#define ISING_KNOB_MSC_WAVES 4
+#define ISING_KNOB_GRAPH_CHUNK 5
+/* Batch and server knobs (ising_batch_set_knob, ising_server_set_knob): ISING_KNOB_BAND is the
+ * longest band a kernel class may use (default 8); ISING_KNOB_ITEMS_PER_SLOT the work items per
+ * resident block a launch aims at (default 6; smaller items balance better, larger ones cost
+ * less per item). */
+#define ISING_KNOB_ITEMS_PER_SLOT 6
+int ising_set_knob(ising_sim* h, int knob, int value);
+int ising_get_knob(ising_sim* h, int knob, int* value);
+
+/* n_sweeps unmeasured sweeps from sweep counter t0, timed on the device with CUDA events on the
+ * handle's stream; blocks until done and returns the elapsed milliseconds in *ms.  Used by the
+ * autotuner; the sweeps are real (the lattice advances).  No counterpart in the reference. */
+int ising_time_sweeps(ising_sim* h, uint64_t t0, int64_t n_sweeps, float* ms);
 
 /* Exact magnetisation M = sum s and energy E = -sum_<ij> s_i s_j (blocks until done).
  * Replaces: observables / magnetization / energy (src/pyising/backends/base.py:125-135;
@@ -209,6 +241,11 @@ int ising_batch_status(ising_batch* b, int64_t id, int* state, int64_t* sweeps_d
 /* Results of a done job: series (n_sweeps / measure_every pairs of (M, E)), final lattice. */
 int ising_batch_result(ising_batch* b, int64_t id, int64_t* series_out, int8_t* lattice_out);
 int ising_batch_release(ising_batch* b, int64_t id);
+/* Launch knobs of a batch (ISING_KNOB_BAND cap, ISING_KNOB_ITEMS_PER_SLOT), applied at the next
+ * rebuild of its work list; identical results for every value.  No counterpart in the reference
+ * (it has no batch). */
+int ising_batch_set_knob(ising_batch* b, int knob, int value);
+int ising_batch_get_knob(ising_batch* b, int knob, int* value);
 int ising_batch_destroy(ising_batch* b);
 
 typedef struct ising_server ising_server;
@@ -227,6 +264,8 @@ int ising_server_release(ising_server* s, int64_t id);
 int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int64_t* used_bytes,
                         int64_t* epoch);
 /* Finish the jobs already submitted, stop the thread and free everything. */
+/* The batch knobs of a server's engine (see ising_batch_set_knob). */
+int ising_server_set_knob(ising_server* s, int knob, int value);
 int ising_server_destroy(ising_server* s);
 
 /* ---- device probes (roofline ceilings and generator checks) ---------------------------- */

@@ -29,6 +29,7 @@ SIGNATURES: dict[str, tuple] = {
     "ising_last_error": (ctypes.c_char_p, []),
     "ising_version": (I, []),
     "ising_device_count": (I, [ctypes.POINTER(I)]),
+    "ising_device_name": (I, [I, ctypes.c_char_p, I]),
     "ising_create": (I, [I, PI64, I, I, U64, I, ctypes.POINTER(P)]),
     "ising_destroy": (I, [P]),
     "ising_set_stream": (I, [P, P]),
@@ -48,6 +49,9 @@ SIGNATURES: dict[str, tuple] = {
     "ising_sweep_static": (I, [I, PI64, I, I, U64, P, I, P, P, U64, I64, I64, P, P]),
     "ising_fill_philox": (I, [P, U64]),
     "ising_set_schedule": (I, [P, I, I]),
+    "ising_set_knob": (I, [P, I, I]),
+    "ising_get_knob": (I, [P, I, ctypes.POINTER(I)]),
+    "ising_time_sweeps": (I, [P, U64, I64, ctypes.POINTER(ctypes.c_float)]),
     "ising_selftest_bounded_wait": (I, [I, ctypes.POINTER(I)]),
     "ising_batch_create": (I, [I, I64, ctypes.POINTER(P)]),
     "ising_batch_add": (I, [P, P, PI64]),
@@ -55,8 +59,11 @@ SIGNATURES: dict[str, tuple] = {
     "ising_batch_status": (I, [P, I64, ctypes.POINTER(I), PI64]),
     "ising_batch_result": (I, [P, I64, P, P]),
     "ising_batch_release": (I, [P, I64]),
+    "ising_batch_set_knob": (I, [P, I, I]),
+    "ising_batch_get_knob": (I, [P, I, ctypes.POINTER(I)]),
     "ising_batch_destroy": (I, [P]),
     "ising_server_create": (I, [I, I64, ctypes.POINTER(P)]),
+    "ising_server_set_knob": (I, [P, I, I]),
     "ising_server_submit": (I, [P, P, PI64]),
     "ising_server_wait": (I, [P, I64, ctypes.c_double, ctypes.POINTER(I)]),
     "ising_server_result": (I, [P, I64, P, P, PD]),

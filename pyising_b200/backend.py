@@ -38,6 +38,10 @@ class _B200Simulation(IsingSimulation):
                                  _lib.ALGORITHM[self.algorithm], self.seed, self.device,
                                  ctypes.byref(self._h)), "create")
         self._upload_table()
+        # launch knobs picked by the autotuner for this GPU and shape, if any (speed only)
+        from . import autotune
+
+        autotune.apply_cached(self)
 
     def __del__(self) -> None:
         h = getattr(self, "_h", None)

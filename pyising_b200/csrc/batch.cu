@@ -30,18 +30,13 @@
 
 namespace ising {
 
+// One msc lattice of a batch (read from global memory by the msc kernel).
 struct BatchLattice {
     void* c[2];
     long long* series;     // (M, E) pairs, or nullptr
     long long join_epoch;  // even epoch of the first half-sweep
-    int variant;
-    int ndim;
-    int rows, lh, ly, lz, cpr, nw, nw_shift;
-    int pitch;             // int8: bytes between rows (lh rounded up to 16)
-    u64 nw_magic;          // msc: ceil(2^64 / nw)
-    int band, bpp;         // int8: rows per band and bands per plane (band schedule)
-    u32 cpr_magic;         // int8: fast_div magic of cpr (0: divide)
-    u32 bpp_magic;         // int8 3D: fast_div magic of bpp (0: divide)
+    int rows, nw, nw_shift;
+    u64 nw_magic;          // ceil(2^64 / nw)
     int every;             // measurement interval in sweeps (0 = none)
     u32 t0;
     u32 k0, k1;
@@ -53,35 +48,63 @@ struct BatchLattice {
 // GPU), within these bounds; both are multiples of 256 chunks or words.
 constexpr long long kInt8ItemMin = 512, kInt8ItemMax = 4096;    // band slots
 constexpr long long kMscItemMin = 2048, kMscItemMax = 16384;    // words
-constexpr long long kItemsPerSlot = 6;
+constexpr long long kItemsPerSlot = 6;  // default of the ISING_KNOB_ITEMS_PER_SLOT knob
+constexpr int kBandCap = 8;             // default of the ISING_KNOB_BAND knob (batch)
 
-// Item size for `total` units of work over `slots` resident blocks.
-inline long long item_size(long long total, long long slots, long long lo, long long hi)
+// Item size for `total` units of work over `slots` resident blocks, `per_slot` items each.
+inline long long item_size(long long total, long long slots, long long per_slot, long long lo,
+                           long long hi)
 {
-    long long want = (total + kItemsPerSlot * slots - 1) / (kItemsPerSlot * slots);
+    long long want = (total + per_slot * slots - 1) / (per_slot * slots);
     return want < lo ? lo : (want > hi ? hi : want);
 }
 
-struct BatchItem {
-    int lat;
-    int pad;
-    long long begin, end;  // band slots band * cpr + jc (int8) or words (msc)
+// ----------------------------------------------------------------------------- int8 -------
+// An int8 launch covers up to kInt8PerLaunch lattices of one kernel class; their descriptors are
+// the launch's parameter block (constant memory), so every field a block reads is uniform, as
+// in the single-lattice kernel.  Block b belongs to the last lattice whose block_begin <= b (a
+// uniform binary search) and updates its slots [(b - block_begin) * per, ...), a slot being a
+// band of L.band rows of one plane in one chunk column (int8_band), band-major.
+struct Int8Desc {
+    void* c[2];
+    long long* series;     // (M, E) pairs, or nullptr
+    long long join_epoch;  // even epoch of the first half-sweep
+    int every;             // measurement interval in sweeps (0 = none)
+    u32 t0, k0, k1;
+    u32 table[7];
+    int rows, lh, ly, lz, pitch, cpr, band, bpp;
+    u32 cpr_magic, bpp_magic;  // fast_div magics of cpr and bpp
+    int block_begin;           // first block of this lattice in the launch
+    int per_block;             // band slots per block (a multiple of 256)
+    int nslots;                // band slots of the lattice: lz * bpp * cpr
 };
 
-// The slots [item.begin, item.end) of one lattice, 256 threads: slot = band * cpr + jc, a band
-// being L.band rows of one plane that the thread walks top to bottom (int8_band).
+// Parameter blocks come in three capacities; a launch passes the smallest that holds its
+// lattices, since the host cost of a launch grows with the size of its parameters.
+constexpr int kInt8PerLaunch = 240;
+
+template <int N>
+struct Int8LaunchN {
+    long long epoch;
+    int n;  // lattices
+    int pad;
+    Int8Desc lat[N];
+};
+using Int8Launch = Int8LaunchN<kInt8PerLaunch>;
+static_assert(sizeof(Int8Launch) <= 32764, "kernel parameter block over the 32 KB limit");
+
 template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
-__device__ __forceinline__ void batch_int8_item(const Int8Half& p, const BatchLattice& L,
-                                                const BatchItem& item, const u32* stab,
-                                                long long& m_acc, long long& e_acc)
+__device__ __forceinline__ void batch_int8_slots(const Int8Half& p, const Int8Desc& L, u32 s0,
+                                                 u32 s1, const u32* stab, long long& m_acc,
+                                                 long long& e_acc)
 {
-    const u32 cpr = (u32)L.cpr, cpr_m = L.cpr_magic, bpp = (u32)L.bpp, bpp_m = L.bpp_magic;
-    for (u32 slot = (u32)item.begin + threadIdx.x; slot < (u32)item.end; slot += 256u) {
-        const u32 band = fast_div(slot, cpr, cpr_m);
+    const u32 cpr = (u32)L.cpr, bpp = (u32)L.bpp;
+    for (u32 slot = s0 + threadIdx.x; slot < s1; slot += 256u) {
+        const u32 band = fast_div(slot, cpr, L.cpr_magic);
         const int j0 = (int)(slot - band * cpr) * V;
         int z = 0, yb = (int)band;
         if constexpr (NDIM == 3) {
-            z = (int)fast_div(band, bpp, bpp_m);
+            z = (int)fast_div(band, bpp, L.bpp_magic);
             yb = (int)(band - (u32)z * bpp);
         }
         const int y0 = yb * L.band;
@@ -90,65 +113,69 @@ __device__ __forceinline__ void batch_int8_item(const Int8Half& p, const BatchLa
     }
 }
 
-// One colour of every lattice of a kernel class.  A block walks its items grid-stride; an item
-// is a run of a lattice's band slots (band-major), so all 256 threads have a slot whatever the
-// row length.
-template <int V, int NDIM, int RULE, bool MIXED>
-// Two resident blocks per SM (up to 128 registers): the lattice parameters of an item live in
-// registers here (they are kernel parameters in the single-lattice kernel), and three blocks
-// per SM (80 registers) spilled and measured slower.
 #ifndef ISING_BATCH_MIN_BLOCKS
-#define ISING_BATCH_MIN_BLOCKS 2
+#define ISING_BATCH_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(256, ISING_BATCH_MIN_BLOCKS) batch_int8_kernel(const BatchLattice* __restrict__ lats,
-                                                         const BatchItem* __restrict__ items,
-                                                         int n_items, long long epoch)
+template <int V, int NDIM, int RULE, bool MIXED, int N>
+__global__ void __launch_bounds__(256, ISING_BATCH_MIN_BLOCKS)
+    batch_int8_kernel(const __grid_constant__ Int8LaunchN<N> P)
 {
-    __shared__ u32 stab[8];  // this item's acceptance table for the per-site lookup rules
-    constexpr bool kLookup = RULE != kMetroFast;
-    const u32 color = (u32)(epoch & 1);
-    // (M, E) sums of the block's consecutive items of one lattice, added to the lattice's
-    // accumulators once, when the block's next item belongs to another lattice or it has none
-    // (one pair of same-address atomics per block and lattice instead of per item)
-    long long m_acc = 0, e_acc = 0;
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BatchItem item = items[it];
-        const BatchLattice& L = lats[item.lat];
-        if constexpr (kLookup) {
-            if (threadIdx.x < 7) stab[threadIdx.x] = L.table[threadIdx.x];
-            __syncthreads();
-        }
-        const u32 s = (u32)((epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
-        const bool meas = color == 1 && L.every > 0 && ((s + 1u) % (u32)L.every) == 0;
-        Int8Half p;
-        p.own = static_cast<int8_t*>(L.c[color]);
-        p.other = static_cast<const int8_t*>(L.c[color ^ 1]);
-        p.rows = L.rows;
-        p.lh = L.lh;
-        p.ly = L.ly;
-        p.lz = L.lz;
-        p.cpr = L.cpr;
-        p.pitch = L.pitch;
-        p.vw = V;
-        p.t = L.t0 + s;
-        p.color = color;
-        p.k0 = L.k0;
-        p.k1 = L.k1;
+    __shared__ u32 stab[8];  // acceptance table for the per-site lookup rules
+    const int b = (int)blockIdx.x;
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.lat[mid].block_begin <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const Int8Desc& L = P.lat[lo];
+    if constexpr (RULE != kMetroFast) {
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int i = 0; i < 7; ++i) p.table[i] = L.table[i];
-        p.meas = meas ? reinterpret_cast<unsigned long long*>(
-                            L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
-                      : nullptr;
-        p.ctl = nullptr;
-        if (meas) batch_int8_item<V, NDIM, RULE, MIXED, true>(p, L, item, stab, m_acc, e_acc);
-        else batch_int8_item<V, NDIM, RULE, MIXED, false>(p, L, item, stab, m_acc, e_acc);
-        if (meas && (it + (int)gridDim.x >= n_items || items[it + gridDim.x].lat != item.lat)) {
-            block_accumulate2(m_acc, e_acc, p.meas);
-            m_acc = e_acc = 0;
+            for (int i = 0; i < 7; ++i) stab[i] = L.table[i];
         }
-        if constexpr (kLookup) __syncthreads();  // stab is rewritten by the next item
+        __syncthreads();
+    }
+    const u32 color = (u32)(P.epoch & 1);
+    const u32 s = (u32)((P.epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
+    const bool meas = color == 1 && L.every > 0 && ((s + 1u) % (u32)L.every) == 0;
+    Int8Half p;
+    p.own = static_cast<int8_t*>(L.c[color]);
+    p.other = static_cast<const int8_t*>(L.c[color ^ 1]);
+    p.rows = L.rows;
+    p.lh = L.lh;
+    p.ly = L.ly;
+    p.lz = L.lz;
+    p.cpr = L.cpr;
+    p.pitch = L.pitch;
+    p.vw = V;
+    p.t = L.t0 + s;
+    p.color = color;
+    p.k0 = L.k0;
+    p.k1 = L.k1;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) p.table[i] = L.table[i];
+    p.meas = meas ? reinterpret_cast<unsigned long long*>(
+                        L.series + 2 * ((s + 1u) / (u32)L.every - 1u))
+                  : nullptr;
+    p.ctl = nullptr;
+    const u32 s0 = (u32)(b - L.block_begin) * (u32)L.per_block;
+    const u32 s1 = s0 + (u32)L.per_block < (u32)L.nslots ? s0 + (u32)L.per_block : (u32)L.nslots;
+    long long m_acc = 0, e_acc = 0;
+    if (meas) {
+        batch_int8_slots<V, NDIM, RULE, MIXED, true>(p, L, s0, s1, stab, m_acc, e_acc);
+        block_accumulate2(m_acc, e_acc, p.meas);
+    } else {
+        batch_int8_slots<V, NDIM, RULE, MIXED, false>(p, L, s0, s1, stab, m_acc, e_acc);
     }
 }
+
+// ------------------------------------------------------------------------------ msc -------
+struct BatchItem {
+    int lat;
+    int pad;
+    long long begin, end;  // words
+};
 
 constexpr int kBatchWarps = 8;
 
@@ -321,9 +348,16 @@ public:
             int rc = rebuild();
             if (rc != ISING_OK) return rc;
         }
+        for (auto& cl : int8_launches_) {
+            for (Int8Launch& P : cl.second) {
+                P.epoch = epoch_;
+                e = launch_int8(cl.first, P);
+                if (e != cudaSuccess) return cuda_fail(e, "batch launch (int8)");
+            }
+        }
         for (const auto& cl : classes_) {
-            e = launch_class(cl.first, cl.second.first, cl.second.second);
-            if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+            e = launch_msc(cl.second.first, cl.second.second);
+            if (e != cudaSuccess) return cuda_fail(e, "batch launch (msc)");
         }
         ++epoch_;
         if ((epoch_ & 1) == 0) {
@@ -407,6 +441,32 @@ public:
 
     int64_t budget() const { return budget_; }
     cudaStream_t stream() const { return stream_; }
+
+    // Launch knobs of the batch (identical results for every value); applied at the next
+    // rebuild of the work list.
+    int set_knob(int knob, int value)
+    {
+        if (knob == ISING_KNOB_BAND) {
+            if (value < 1 || value > 64) return fail(ISING_ERR_INVALID, "band cap must be 1..64");
+            band_cap_ = value;
+        } else if (knob == ISING_KNOB_ITEMS_PER_SLOT) {
+            if (value < 1 || value > 64)
+                return fail(ISING_ERR_INVALID, "items per slot must be 1..64");
+            items_per_slot_ = value;
+        } else {
+            return fail(ISING_ERR_INVALID, "knob %d does not apply to a batch", knob);
+        }
+        dirty_ = true;
+        return ISING_OK;
+    }
+
+    int get_knob(int knob, int* value) const
+    {
+        if (knob == ISING_KNOB_BAND) *value = band_cap_;
+        else if (knob == ISING_KNOB_ITEMS_PER_SLOT) *value = (int)items_per_slot_;
+        else return fail(ISING_ERR_INVALID, "knob %d does not apply to a batch", knob);
+        return ISING_OK;
+    }
 
 private:
     int validate(const ising_job& s, Job& j)
@@ -521,86 +581,114 @@ private:
         return ISING_OK;
     }
 
-    // Builds the lattice table and the work items, grouped by kernel class.
+    // Builds the launch lists, grouped by kernel class: for int8 classes the lattice
+    // descriptors of each launch (chunks of kInt8PerLaunch), for msc the lattice table and the
+    // work items in device memory.
     int rebuild()
     {
-        std::vector<BatchLattice> lats;
-        std::vector<KernelClass> lat_class;
-        std::map<KernelClass, long long> class_units;  // sites (int8) or words (msc) per class
-        lats.reserve(active_.size());
+        std::vector<BatchLattice> lats;              // msc lattices
+        std::map<KernelClass, std::vector<Int8Desc>> int8_descs;
+        std::map<KernelClass, long long> class_units;  // chunk-rows (int8) or words (msc)
+        std::vector<std::pair<KernelClass, int>> msc_of;  // (class, index in lats)
         for (int64_t id : active_) {
             Job& j = *jobs_[id];
             const ising_job& s = j.spec;
-            BatchLattice L;
-            memset(&L, 0, sizeof L);
-            L.c[0] = j.c[0];
-            L.c[1] = j.c[1];
-            L.series = j.d_series;
-            L.join_epoch = j.join_epoch;
-            L.variant = s.variant;
-            L.ndim = s.ndim;
-            L.rows = j.rows;
-            L.lh = j.lh;
-            L.ly = j.ly;
-            L.lz = j.lz;
-            L.nw = j.nw;
-            L.nw_shift = s.variant == ISING_VARIANT_MSC && (j.nw & (j.nw - 1)) == 0
-                             ? __builtin_ctz((unsigned)j.nw) : -1;
-            L.nw_magic = magic_for(j.nw);
-            L.every = (int)s.measure_every;
-            L.t0 = (u32)s.t0;
-            L.k0 = (u32)s.seed;
-            L.k1 = (u32)(s.seed >> 32);
-            for (int i = 0; i < 7; ++i) L.table[i] = i < s.table_n ? s.table[i] : 0xFFFFFFFFu;
+            u32 table[7];
+            for (int i = 0; i < 7; ++i) table[i] = i < s.table_n ? s.table[i] : 0xFFFFFFFFu;
             KernelClass kc{s.variant, 0, s.ndim, 0, 0};
             if (s.variant == ISING_VARIANT_MSC) {
+                BatchLattice L;
+                memset(&L, 0, sizeof L);
+                L.c[0] = j.c[0];
+                L.c[1] = j.c[1];
+                L.series = j.d_series;
+                L.join_epoch = j.join_epoch;
+                L.rows = j.rows;
+                L.nw = j.nw;
+                L.nw_shift = (j.nw & (j.nw - 1)) == 0 ? __builtin_ctz((unsigned)j.nw) : -1;
+                L.nw_magic = magic_for(j.nw);
+                L.every = (int)s.measure_every;
+                L.t0 = (u32)s.t0;
+                L.k0 = (u32)s.seed;
+                L.k1 = (u32)(s.seed >> 32);
+                memcpy(L.table, table, sizeof table);
                 class_units[kc] += (long long)j.rows * j.nw;
+                msc_of.emplace_back(kc, (int)lats.size());
+                lats.push_back(L);
             } else {
-                const int v = 16;  // rows padded to 16 bytes
-                L.pitch = j.pitch;
-                L.cpr = (j.lh + v - 1) / v;
-
-                kc.v = v;
-                kc.mixed = (j.lh % v) != 0;
-                kc.rule = select_rule(s.variant, s.algorithm, s.ndim, L.table);
-                class_units[kc] += (long long)j.rows * L.cpr;
+                Int8Desc D;
+                memset(&D, 0, sizeof D);
+                D.c[0] = j.c[0];
+                D.c[1] = j.c[1];
+                D.series = j.d_series;
+                D.join_epoch = j.join_epoch;
+                D.every = (int)s.measure_every;
+                D.t0 = (u32)s.t0;
+                D.k0 = (u32)s.seed;
+                D.k1 = (u32)(s.seed >> 32);
+                memcpy(D.table, table, sizeof table);
+                D.rows = j.rows;
+                D.lh = j.lh;
+                D.ly = j.ly;
+                D.lz = j.lz;
+                D.pitch = j.pitch;  // rows padded to 16 bytes: chunk width 16
+                D.cpr = (j.lh + 15) / 16;
+                kc.v = 16;
+                kc.mixed = (j.lh % 16) != 0;
+                kc.rule = select_rule(s.variant, s.algorithm, s.ndim, table);
+                class_units[kc] += (long long)j.rows * D.cpr;
+                int8_descs[kc].push_back(D);
             }
-            lats.push_back(L);
-            lat_class.push_back(kc);
         }
-        std::map<KernelClass, std::vector<BatchItem>> by_class;
-        std::map<KernelClass, int> class_band;
-        for (int li = 0; li < (int)lats.size(); ++li) {
-            const BatchLattice& L = lats[li];
-            const KernelClass& kc = lat_class[li];
+        // int8: the class's band height is the longest power of two up to the band cap that
+        // still leaves items_per_slot blocks of one slot per thread per resident block; blocks
+        // of a lattice hold per_block slots, sized the same way
+        int8_launches_.clear();
+        for (auto& kv : int8_descs) {
+            const KernelClass& kc = kv.first;
             const long long units = class_units[kc];
-            std::vector<BatchItem>& out = by_class[kc];
-            if (L.variant == ISING_VARIANT_MSC) {
-                const long long words = (long long)L.rows * L.nw;
-                long long per = item_size(units, slots(kc), kMscItemMin, kMscItemMax);
-                per = (per + 255) / 256 * 256;
-                for (long long b = 0; b < words; b += per)
-                    out.push_back(BatchItem{li, 0, b, std::min(words, b + per)});
-            } else {
-                // the class's band height: the longest of 8, 4, 2, 1 rows that still leaves
-                // kItemsPerSlot items of one slot per thread for every resident block
-                int& band = class_band[kc];
-                if (band == 0) {
-                    const long long want = kItemsPerSlot * 256 * slots(kc);
-                    band = 8;
-                    while (band > 1 && units / band < want) band >>= 1;
+            const long long want = items_per_slot_ * 256 * slots(kc);
+            int band = 1;
+            while (band * 2 <= band_cap_) band *= 2;
+            while (band > 1 && units / band < want) band >>= 1;
+            long long per = item_size(units / band, slots(kc), items_per_slot_, kInt8ItemMin,
+                                      kInt8ItemMax);
+            per = (per + 255) / 256 * 256;
+            std::vector<Int8Launch> launches;
+            for (size_t i = 0; i < kv.second.size(); ++i) {
+                if (i % kInt8PerLaunch == 0) {
+                    launches.emplace_back();
+                    memset(&launches.back(), 0, sizeof(Int8Launch));
                 }
-                BatchLattice& M = lats[li];
-                M.band = band < M.ly ? band : M.ly;
-                M.bpp = (M.ly + M.band - 1) / M.band;
-                const long long nslots = (long long)M.lz * M.bpp * M.cpr;
-                M.cpr_magic = fast_div_magic((u32)M.cpr, (unsigned long long)nslots);
-                M.bpp_magic = fast_div_magic((u32)M.bpp, (unsigned long long)M.lz * M.bpp);
-                long long per = item_size(units / M.band, slots(kc), kInt8ItemMin, kInt8ItemMax);
-                per = (per + 255) / 256 * 256;
-                for (long long b = 0; b < nslots; b += per)
-                    out.push_back(BatchItem{li, 0, b, std::min(nslots, b + per)});
+                Int8Launch& P = launches.back();
+                Int8Desc D = kv.second[i];
+                D.band = band < D.ly ? band : D.ly;
+                D.bpp = (D.ly + D.band - 1) / D.band;
+                const long long nslots = (long long)D.lz * D.bpp * D.cpr;
+                D.nslots = (int)nslots;
+                D.cpr_magic = fast_div_magic((u32)D.cpr, (unsigned long long)nslots);
+                D.bpp_magic = fast_div_magic((u32)D.bpp, (unsigned long long)D.lz * D.bpp);
+                D.per_block = (int)per;
+                const int prev = P.n ? P.lat[P.n - 1].block_begin +
+                                           (P.lat[P.n - 1].nslots + P.lat[P.n - 1].per_block - 1) /
+                                               P.lat[P.n - 1].per_block
+                                     : 0;
+                D.block_begin = prev;
+                P.lat[P.n++] = D;
             }
+            int8_launches_.emplace_back(kc, std::move(launches));
+        }
+        // msc: work items of whole 256-word runs over the class's lattices
+        std::map<KernelClass, std::vector<BatchItem>> by_class;
+        for (const auto& m : msc_of) {
+            const KernelClass& kc = m.first;
+            const BatchLattice& L = lats[m.second];
+            const long long words = (long long)L.rows * L.nw;
+            long long per = item_size(class_units[kc], slots(kc), items_per_slot_, kMscItemMin,
+                                      kMscItemMax);
+            per = (per + 255) / 256 * 256;
+            for (long long b = 0; b < words; b += per)
+                by_class[kc].push_back(BatchItem{m.second, 0, b, std::min(words, b + per)});
         }
         std::vector<BatchItem> items;
         classes_.clear();
@@ -615,12 +703,20 @@ private:
         return rc;
     }
 
+    // Blocks of an int8 launch: the last lattice's block_begin plus its blocks.
+    static unsigned int8_grid(const Int8Launch& P)
+    {
+        const Int8Desc& L = P.lat[P.n - 1];
+        return (unsigned)(L.block_begin + (L.nslots + L.per_block - 1) / L.per_block);
+    }
+
     // Resident blocks of a class's kernel on the whole device.
     long long slots(const KernelClass& kc)
     {
         const void* fn = kc.variant == ISING_VARIANT_MSC
                              ? (const void*)batch_msc_kernel
-                             : (const void*)batch_int8_kernel<16, 2, kMetroFast, false>;
+                             : (const void*)batch_int8_kernel<16, 2, kMetroFast, false, 16>;
+        // (one occupancy for all int8 classes: they share the launch bounds)
         return (long long)sms_ * blocks_per_sm(fn, kc.variant == ISING_VARIANT_MSC
                                                        ? kBatchWarps * 32 : 256);
     }
@@ -659,42 +755,54 @@ private:
         return n_items < g ? n_items : g;
     }
 
-    template <int V, int NDIM, bool MIXED>
-    cudaError_t launch_int8_rule(int rule, const BatchItem* it, int n)
+    template <int V, int NDIM, bool MIXED, int N>
+    cudaError_t launch_int8_cap(int rule, const Int8Launch& full)
     {
+        Int8LaunchN<N> P;
+        P.epoch = full.epoch;
+        P.n = full.n;
+        P.pad = 0;
+        memcpy(P.lat, full.lat, (size_t)full.n * sizeof(Int8Desc));
+        const unsigned grid = int8_grid(full);
         switch (rule) {
-#define ISING_BATCH_CASE(R)                                                                   \
-    case R: {                                                                                 \
-        auto fn = batch_int8_kernel<V, NDIM, R, MIXED>;                                        \
-        fn<<<grid_for((const void*)fn, n), 256, 0, stream_>>>(d_lats_, it, n, epoch_);        \
-        break;                                                                                \
-    }
-            ISING_BATCH_CASE(kMetroFast)
-            ISING_BATCH_CASE(kHeatFast)
-            ISING_BATCH_CASE(kMetroGeneric)
-            ISING_BATCH_CASE(kHeatGeneric)
-#undef ISING_BATCH_CASE
+        case kMetroFast: batch_int8_kernel<V, NDIM, kMetroFast, MIXED, N><<<grid, 256, 0, stream_>>>(P); break;
+        case kHeatFast: batch_int8_kernel<V, NDIM, kHeatFast, MIXED, N><<<grid, 256, 0, stream_>>>(P); break;
+        case kMetroGeneric:
+            batch_int8_kernel<V, NDIM, kMetroGeneric, MIXED, N><<<grid, 256, 0, stream_>>>(P);
+            break;
+        case kHeatGeneric:
+            batch_int8_kernel<V, NDIM, kHeatGeneric, MIXED, N><<<grid, 256, 0, stream_>>>(P);
+            break;
         default: return cudaErrorInvalidValue;
         }
         return cudaGetLastError();
     }
 
-    cudaError_t launch_class(const KernelClass& kc, int off, int n)
+    template <int V, int NDIM, bool MIXED>
+    cudaError_t launch_int8_rule(int rule, const Int8Launch& P)
     {
-        const BatchItem* it = d_items_ + off;
-        if (kc.variant == ISING_VARIANT_MSC) {
-            auto fn = batch_msc_kernel;
-            fn<<<grid_for((const void*)fn, n, kBatchWarps * 32), kBatchWarps * 32, 0, stream_>>>(d_lats_, it, n,
-                                                                               epoch_);
-            return cudaGetLastError();
-        }
-        // int8 rows are padded to 16 bytes, so the chunk width is always 16; lattices whose rows
-        // are a multiple of 16 get the kernel without the partial-chunk code.
+        if (P.n <= 16) return launch_int8_cap<V, NDIM, MIXED, 16>(rule, P);
+        if (P.n <= 64) return launch_int8_cap<V, NDIM, MIXED, 64>(rule, P);
+        return launch_int8_cap<V, NDIM, MIXED, kInt8PerLaunch>(rule, P);
+    }
+
+    // int8 rows are padded to 16 bytes, so the chunk width is always 16; lattices whose rows are
+    // a multiple of 16 get the kernel without the partial-chunk code.
+    cudaError_t launch_int8(const KernelClass& kc, const Int8Launch& P)
+    {
         if (kc.ndim == 3)
-            return kc.mixed ? launch_int8_rule<16, 3, true>(kc.rule, it, n)
-                            : launch_int8_rule<16, 3, false>(kc.rule, it, n);
-        return kc.mixed ? launch_int8_rule<16, 2, true>(kc.rule, it, n)
-                        : launch_int8_rule<16, 2, false>(kc.rule, it, n);
+            return kc.mixed ? launch_int8_rule<16, 3, true>(kc.rule, P)
+                            : launch_int8_rule<16, 3, false>(kc.rule, P);
+        return kc.mixed ? launch_int8_rule<16, 2, true>(kc.rule, P)
+                        : launch_int8_rule<16, 2, false>(kc.rule, P);
+    }
+
+    cudaError_t launch_msc(int off, int n)
+    {
+        auto fn = batch_msc_kernel;
+        fn<<<grid_for((const void*)fn, n, kBatchWarps * 32), kBatchWarps * 32, 0, stream_>>>(
+            d_lats_, d_items_ + off, n, epoch_);
+        return cudaGetLastError();
     }
 
     int retire()
@@ -855,6 +963,8 @@ private:
     std::multimap<size_t, void*> pinned_free_;  // reusable pinned result buffers by size class
     long long epoch_ = 0;
     int64_t last_id_ = 0;
+    int band_cap_ = kBandCap;
+    long long items_per_slot_ = kItemsPerSlot;
     std::map<int64_t, std::unique_ptr<Job>> jobs_;
     std::deque<int64_t> pending_;
     std::vector<int64_t> active_;
@@ -863,7 +973,8 @@ private:
     BatchLattice* d_lats_ = nullptr;
     BatchItem* d_items_ = nullptr;
     size_t lats_cap_ = 0, items_cap_ = 0;
-    std::vector<std::pair<KernelClass, std::pair<int, int>>> classes_;
+    std::vector<std::pair<KernelClass, std::pair<int, int>>> classes_;  // msc work items
+    std::vector<std::pair<KernelClass, std::vector<Int8Launch>>> int8_launches_;
     std::vector<cudaEvent_t> epoch_events_, free_events_;
     std::map<const void*, int> occupancy_;
     std::deque<cudaEvent_t> inflight_;
@@ -952,6 +1063,18 @@ int ising_batch_release(ising_batch* b, int64_t id)
 {
     if (!b) return fail(ISING_ERR_INVALID, "null batch");
     return b->eng->release(id);
+}
+
+int ising_batch_set_knob(ising_batch* b, int knob, int value)
+{
+    if (!b) return fail(ISING_ERR_INVALID, "null batch");
+    return b->eng->set_knob(knob, value);
+}
+
+int ising_batch_get_knob(ising_batch* b, int knob, int* value)
+{
+    if (!b || !value) return fail(ISING_ERR_INVALID, "null argument");
+    return b->eng->get_knob(knob, value);
 }
 
 int ising_batch_destroy(ising_batch* b)
@@ -1093,6 +1216,13 @@ int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int6
     if (used_bytes) *used_bytes = s->eng->used_bytes();
     if (epoch) *epoch = s->eng->epoch();
     return ISING_OK;
+}
+
+int ising_server_set_knob(ising_server* s, int knob, int value)
+{
+    if (!s) return fail(ISING_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->eng->set_knob(knob, value);
 }
 
 int ising_server_destroy(ising_server* s)

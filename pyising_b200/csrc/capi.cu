@@ -54,8 +54,8 @@ int select_rule(int variant, int algorithm, int ndim, const u32* table)
 
 namespace ising {
 
-// Sweeps per captured chunk without measurements; longest chunk captured at all.
-constexpr int64_t kGraphChunk = 32;
+// Longest chunk of sweeps captured in one graph (the chunk length of unmeasured runs is the
+// handle's graph_chunk knob, 32 by default).
 constexpr int64_t kGraphChunkMax = 256;
 
 // Reads the error word of the last persistent run (waits for the handle's stream).
@@ -155,6 +155,20 @@ extern "C" {
 const char* ising_last_error(void) { return g_last_error.c_str(); }
 
 int ising_version(void) { return 100; }
+
+int ising_device_name(int device, char* buf, int buflen)
+{
+    if (!buf || buflen < 1) return fail(ISING_ERR_INVALID, "null or empty output buffer");
+    cudaDeviceProp prop;
+    const cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "cudaGetDeviceProperties");
+    }
+    snprintf(buf, (size_t)buflen, "%s sm_%d%d %d SMs", prop.name, prop.major, prop.minor,
+             prop.multiProcessorCount);
+    return ISING_OK;
+}
 
 int ising_device_count(int* n)
 {
@@ -456,6 +470,82 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band)
     return ISING_OK;
 }
 
+int ising_set_knob(ising_sim* h, int knob, int value)
+{
+    CHECK_HANDLE(h);
+    switch (knob) {
+    case ISING_KNOB_BAND:
+        if (h->variant != ISING_VARIANT_INT8) return fail(ISING_ERR_INVALID, "band: int8 only");
+        if (value < 0 || value > 1024) return fail(ISING_ERR_INVALID, "band must be 0..1024");
+        h->band = value;
+        break;
+    case ISING_KNOB_CHUNK_WIDTH:
+        if (h->variant != ISING_VARIANT_INT8)
+            return fail(ISING_ERR_INVALID, "chunk width: int8 only");
+        if (value != 16 && value != 8 && value != 4)
+            return fail(ISING_ERR_INVALID, "chunk width must be 16, 8 or 4 bytes");
+        if (value == 8 && h->lh % 8)
+            return fail(ISING_ERR_INVALID, "chunk width 8 needs Lx/2 to be a multiple of 8");
+        h->vw = value;
+        break;
+    case ISING_KNOB_BLOCKS_PER_SM:
+        if (value < 1 || value > 32) return fail(ISING_ERR_INVALID, "blocks per SM must be 1..32");
+        h->blocks_per_sm = value;
+        h->max_blocks = h->sm_count * value;
+        break;
+    case ISING_KNOB_MSC_WAVES:
+        if (value < 1 || value > 16) return fail(ISING_ERR_INVALID, "msc waves must be 1..16");
+        h->msc_waves = value;
+        break;
+    case ISING_KNOB_GRAPH_CHUNK:
+        if (value < 1 || value > kGraphChunkMax)
+            return fail(ISING_ERR_INVALID, "graph chunk must be 1..%d sweeps", (int)kGraphChunkMax);
+        h->graph_chunk = value;
+        break;
+    default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
+    }
+    clear_graphs(h);  // captured graphs hold the old launch parameters
+    return ISING_OK;
+}
+
+int ising_get_knob(ising_sim* h, int knob, int* value)
+{
+    CHECK_HANDLE(h);
+    if (!value) return fail(ISING_ERR_INVALID, "null output pointer");
+    switch (knob) {
+    case ISING_KNOB_BAND: *value = h->band; break;
+    case ISING_KNOB_CHUNK_WIDTH: *value = h->vw; break;
+    case ISING_KNOB_BLOCKS_PER_SM: *value = h->blocks_per_sm; break;
+    case ISING_KNOB_MSC_WAVES: *value = h->msc_waves; break;
+    case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
+    default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
+    }
+    return ISING_OK;
+}
+
+int ising_time_sweeps(ising_sim* h, uint64_t t0, int64_t n_sweeps, float* ms)
+{
+    CHECK_HANDLE(h);
+    if (!ms || n_sweeps <= 0) return fail(ISING_ERR_INVALID, "bad arguments");
+    TRY_CUDA(cudaSetDevice(h->device));
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    int rc = ISING_OK;
+    if (e == cudaSuccess) e = cudaEventRecord(a, h->stream);
+    if (e == cudaSuccess) {
+        rc = ising_sweep(h, t0, n_sweeps, 0, nullptr);
+        if (rc == ISING_OK) e = cudaEventRecord(b, h->stream);
+        if (rc == ISING_OK && e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (rc == ISING_OK && e == cudaSuccess) e = cudaEventElapsedTime(ms, a, b);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (rc != ISING_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "timed sweeps");
+    return ISING_OK;
+}
+
 int ising_selftest_bounded_wait(int device, int* timed_out)
 {
     if (!timed_out) return fail(ISING_ERR_INVALID, "null output pointer");
@@ -517,7 +607,7 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
     }
     // Whole chunks of G sweeps replay one captured graph (G = the measurement interval, so each
     // chunk ends with its measurement); the rest is launched directly.
-    const int64_t G = measure_every > 0 ? measure_every : kGraphChunk;
+    const int64_t G = measure_every > 0 ? measure_every : h->graph_chunk;
     if (h->schedule != ISING_SCHEDULE_LAUNCHES && G <= kGraphChunkMax && n_sweeps >= 2 * G) {
         cudaGraphExec_t exec = nullptr;
         int rc = chunk_graph(h, G, measure_every > 0, &exec);
@@ -723,7 +813,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.meas = meas;
         p.stats = stats;
         p.ctl = ctl;
-        e = launch_msc_half(true, p, h->max_blocks, h->stream);
+        e = launch_msc_half(true, p, h->max_blocks, h->sm_count, h->msc_waves, h->stream);
     } else {
         Int8Half p;
         p.own = (int8_t*)h->c[color];
@@ -743,7 +833,7 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         for (int i = 0; i < 7; ++i) p.table[i] = h->table[i];
         p.meas = meas;
         p.ctl = ctl;
-        e = launch_int8_half(h->ndim, h->rule, p, h->max_blocks, h->stream);
+        e = launch_int8_half(h->ndim, h->rule, p, h->max_blocks, h->sm_count, h->stream);
     }
     if (e != cudaSuccess) return cuda_fail(e, "half-sweep launch");
     return ISING_OK;
@@ -761,7 +851,7 @@ int observe(ising_sim* h, unsigned long long* acc)
         p.nw = h->nw;
         p.color = 1;
         p.meas = acc;
-        e = launch_msc_half(false, p, h->max_blocks, h->stream);
+        e = launch_msc_half(false, p, h->max_blocks, h->sm_count, 1, h->stream);
     } else {
         Int8Half p;
         memset(&p, 0, sizeof p);
@@ -776,7 +866,7 @@ int observe(ising_sim* h, unsigned long long* acc)
         p.cpr = (h->lh + h->vw - 1) / h->vw;
         p.color = 1;
         p.meas = acc;
-        e = launch_int8_half(h->ndim, kObserve, p, h->max_blocks, h->stream);
+        e = launch_int8_half(h->ndim, kObserve, p, h->max_blocks, h->sm_count, h->stream);
     }
     if (e != cudaSuccess) return cuda_fail(e, "observables launch");
     return ISING_OK;

@@ -35,7 +35,11 @@ struct ising_sim {
     long long* h_series = nullptr;        // pinned copy of d_series
     int64_t series_cap = 0;               // pairs
     int sm_count = 148;
-    int max_blocks = 148 * 8;
+    int max_blocks = 148 * 8;           // grid cap: sm_count * blocks_per_sm
+    // Launch knobs (ising_set_knob); every value gives identical results.
+    int blocks_per_sm = 8;
+    int msc_waves = 1;                  // msc: warp ranges per resident warp
+    int64_t graph_chunk = 32;           // sweeps per captured graph of an unmeasured run
     // Captured chunks of `sweeps` sweeps (one measurement at the end when `measured`), replayed
     // with the sweep counter and series slot in d_acc[6], d_acc[7].
     struct Graph {
@@ -71,9 +75,10 @@ int selftest_bounded_wait(int device, int* timed_out);
 int int8_chunk_width(int lh);
 int int8_default_band(long long rows, int ly, int cpr, int sm_count);
 unsigned int8_band_geometry(Int8Half& p, int max_blocks, int sm_count);
-cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_blocks,
+cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_blocks, int sm_count,
                              cudaStream_t st);
-cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st);
+cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int sm_count,
+                            int waves, cudaStream_t st);
 cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,
                               long long row0, int lh, int pitch, int ly, int max_blocks,
                               cudaStream_t st);

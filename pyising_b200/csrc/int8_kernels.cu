@@ -6,7 +6,7 @@
 // band's rows top to bottom (int8_band), so consecutive threads of a warp read consecutive
 // 16-byte chunks of the same rows.  Longer bands reuse more opposite-colour rows but leave fewer
 // slots to fill the GPU; the launcher's default picks the longest band (up to 16 rows) that
-// still gives every SM two waves of resident threads, and a tuned value can replace it.
+// still gives every SM a wave of resident threads, and a tuned value can replace it.
 #include "int8_core.cuh"
 
 namespace ising {
@@ -73,11 +73,11 @@ static cudaError_t launch_v(int ndim, int rule, const Int8Half& p, unsigned grid
 // Chunk width used for a row of lh bytes: the widest of 16/8/4 that divides it.
 int int8_chunk_width(int lh) { return lh % 16 == 0 ? 16 : (lh % 8 == 0 ? 8 : 4); }
 
-// Default band height: the longest of 16, 8, 4, 2, 1 rows whose slots still give every SM two
-// waves of resident threads (4 blocks of 256 at 64 registers).
+// Default band height: the longest of 16, 8, 4, 2, 1 rows whose slots still give every SM one
+// wave of resident threads (4 blocks of 256 at 64 registers).
 int int8_default_band(long long rows, int ly, int cpr, int sm_count)
 {
-    const long long want = 2LL * 1024 * sm_count;
+    const long long want = 1024LL * sm_count;
     int b = 16;
     while (b > 1 && (rows / ly) * ((ly + b - 1) / b) * (long long)cpr < want) b >>= 1;
     return b;
@@ -98,12 +98,11 @@ unsigned int8_band_geometry(Int8Half& p, int max_blocks, int sm_count)
     return (unsigned)(g < 1 ? 1 : g);
 }
 
-cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p_in, int max_blocks,
+cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p_in, int max_blocks, int sm_count,
                              cudaStream_t st)
 {
     Int8Half p = p_in;
-    // callers pass max_blocks = 8 blocks per SM
-    const unsigned grid = int8_band_geometry(p, max_blocks, max_blocks / 8 > 0 ? max_blocks / 8 : 1);
+    const unsigned grid = int8_band_geometry(p, max_blocks, sm_count);
     const int v = p.vw;
     if (v == 16) {  // padded rows (lh % 16 != 0) need the partial-chunk code
         return (p.lh % 16) ? launch_v<16, true>(ndim, rule, p, grid, st)

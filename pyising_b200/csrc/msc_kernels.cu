@@ -87,13 +87,15 @@ static int queue_blocks_per_sm()
 
 int msc_nw_shift(int nw) { return (nw & (nw - 1)) == 0 ? __builtin_ctz((unsigned)nw) : -1; }
 
-cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, cudaStream_t st)
+cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int sm_count,
+                            int waves, cudaStream_t st)
 {
     if (update && !p.stats) {
-        // one resident wave of warps, each with an equal contiguous range of words
+        // `waves` resident waves of warps (one by default), each warp with an equal contiguous
+        // range of words
         const long long total = (long long)p.rows * p.nw;
-        const int sms = max_blocks / 8 > 0 ? max_blocks / 8 : 1;
-        const long long warps = (long long)sms * queue_blocks_per_sm() * kQueueWarps;
+        const long long warps = (long long)(sm_count > 0 ? sm_count : 1) * queue_blocks_per_sm() *
+                                kQueueWarps * (waves > 0 ? waves : 1);
         long long per_warp = (total + warps - 1) / warps;
         per_warp = (per_warp + 31) / 32 * 32;
         if (per_warp < 32) per_warp = 32;

@@ -150,7 +150,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 p.meas = m;
                 p.stats = nullptr;
                 p.ctl = nullptr;
-                e = launch_msc_half(true, p, max_blocks, st);
+                e = launch_msc_half(true, p, max_blocks, max_blocks / 8, 1, st);
             } else {
                 Int8Half p;
                 memset(&p, 0, sizeof p);
@@ -170,7 +170,7 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                 for (int i = 0; i < 7; ++i) p.table[i] = tab[i];
                 p.meas = m;
                 p.ctl = nullptr;
-                e = launch_int8_half(ndim, rule, p, max_blocks, st);
+                e = launch_int8_half(ndim, rule, p, max_blocks, max_blocks / 8, st);
             }
             if (e != cudaSuccess) return cuda_fail(e, "static sweep launch");
         }

@@ -139,6 +139,20 @@ class Ensemble:
         self._jobs[jid.value] = job
         return int(jid.value)
 
+    BATCH_KNOBS = {"band": 1, "items_per_slot": 6}
+
+    def set_knob(self, name: str, value: int) -> None:
+        """Batch launch knob (``"band"``: longest band of a kernel class, ``"items_per_slot"``:
+        work items per resident block); results are identical for every value."""
+        check(lib().ising_batch_set_knob(self._b, self.BATCH_KNOBS[name], int(value)),
+              "batch_set_knob")
+
+    def get_knob(self, name: str) -> int:
+        v = ctypes.c_int()
+        check(lib().ising_batch_get_knob(self._b, self.BATCH_KNOBS[name], ctypes.byref(v)),
+              "batch_get_knob")
+        return int(v.value)
+
     def run(self, max_epochs: int = 0) -> int:
         """Advance until every job is done (or ``max_epochs`` half-sweeps); returns epochs run."""
         n = ctypes.c_int64()
@@ -198,6 +212,11 @@ class Server:
               "server_submit")
         self._jobs[jid.value] = job
         return int(jid.value)
+
+    def set_knob(self, name: str, value: int) -> None:
+        """Batch launch knob of the server's engine (see :meth:`Ensemble.set_knob`)."""
+        check(lib().ising_server_set_knob(self._s, Ensemble.BATCH_KNOBS[name], int(value)),
+              "server_set_knob")
 
     def wait(self, jid: int, timeout: float | None = None) -> str:
         st = ctypes.c_int()
