@@ -121,6 +121,11 @@ __global__ void __launch_bounds__(256, ISING_BATCH_MIN_BLOCKS)
     batch_int8_kernel(const __grid_constant__ Int8LaunchN<N> P)
 {
     __shared__ u32 stab[8];  // acceptance table for the per-site lookup rules
+    // launched with programmatic stream serialization: wait for the previous kernel of the
+    // stream (every kernel of the engine's stream waits on its predecessor in turn, so this
+    // class's previous half-sweep has completed too), then let the next launch start
+    pdl_wait();
+    pdl_trigger();
     const int b = (int)blockIdx.x;
     int lo = 0, hi = P.n - 1;
     while (lo < hi) {
@@ -185,6 +190,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
 {
     __shared__ QueueSlots q_all[kBatchWarps];
     __shared__ uint4 lvmask[16];
+    // (launched without programmatic serialization: its early-launched blocks would hold their
+    // 17 KB work stacks while waiting, and the batch measured slower with it)
     const u32 color = (u32)(epoch & 1);
     const int warp = threadIdx.x >> 5;
     long long m_acc = 0, e_acc = 0;  // flushed per lattice, as in batch_int8_kernel
@@ -763,19 +770,20 @@ private:
         P.n = full.n;
         P.pad = 0;
         memcpy(P.lat, full.lat, (size_t)full.n * sizeof(Int8Desc));
-        const unsigned grid = int8_grid(full);
+        const dim3 grid(int8_grid(full)), block(256);
         switch (rule) {
-        case kMetroFast: batch_int8_kernel<V, NDIM, kMetroFast, MIXED, N><<<grid, 256, 0, stream_>>>(P); break;
-        case kHeatFast: batch_int8_kernel<V, NDIM, kHeatFast, MIXED, N><<<grid, 256, 0, stream_>>>(P); break;
+        case kMetroFast:
+            return launch_pdl(batch_int8_kernel<V, NDIM, kMetroFast, MIXED, N>, grid, block, stream_, P);
+        case kHeatFast:
+            return launch_pdl(batch_int8_kernel<V, NDIM, kHeatFast, MIXED, N>, grid, block, stream_, P);
         case kMetroGeneric:
-            batch_int8_kernel<V, NDIM, kMetroGeneric, MIXED, N><<<grid, 256, 0, stream_>>>(P);
-            break;
+            return launch_pdl(batch_int8_kernel<V, NDIM, kMetroGeneric, MIXED, N>, grid, block,
+                              stream_, P);
         case kHeatGeneric:
-            batch_int8_kernel<V, NDIM, kHeatGeneric, MIXED, N><<<grid, 256, 0, stream_>>>(P);
-            break;
+            return launch_pdl(batch_int8_kernel<V, NDIM, kHeatGeneric, MIXED, N>, grid, block,
+                              stream_, P);
         default: return cudaErrorInvalidValue;
         }
-        return cudaGetLastError();
     }
 
     template <int V, int NDIM, bool MIXED>
@@ -800,8 +808,8 @@ private:
     cudaError_t launch_msc(int off, int n)
     {
         auto fn = batch_msc_kernel;
-        fn<<<grid_for((const void*)fn, n, kBatchWarps * 32), kBatchWarps * 32, 0, stream_>>>(
-            d_lats_, d_items_ + off, n, epoch_);
+        const dim3 grid(grid_for((const void*)fn, n, kBatchWarps * 32)), block(kBatchWarps * 32);
+        fn<<<grid, block, 0, stream_>>>(d_lats_, d_items_ + off, n, epoch_);
         return cudaGetLastError();
     }
 

@@ -55,8 +55,11 @@ int select_rule(int variant, int algorithm, int ndim, const u32* table)
 namespace ising {
 
 // Longest chunk of sweeps captured in one graph (the chunk length of unmeasured runs is the
-// handle's graph_chunk knob, 32 by default).
+// handle's graph_chunk knob, 32 by default); shortest remainder of a call replayed as a graph;
+// graphs a handle keeps before remainders are launched directly.
 constexpr int64_t kGraphChunkMax = 256;
+constexpr int64_t kGraphRemainderMin = 4;
+constexpr size_t kGraphsKept = 16;
 
 // Reads the error word of the last persistent run (waits for the handle's stream).
 static int check_pending(ising_sim* h)
@@ -618,6 +621,17 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
         for (int64_t c = 0; c < chunks; ++c) TRY_CUDA(cudaGraphLaunch(exec, h->stream));
         s0 = chunks * G;
         k = measure_every > 0 ? chunks : 0;
+        // the rest (no measurement falls in it) as one more graph, captured once per length
+        // and kept while the handle holds few graphs: a repeated call then issues no single
+        // launches at all
+        const int64_t rem = n_sweeps - s0;
+        if (rem >= kGraphRemainderMin && h->graphs.size() < kGraphsKept) {
+            cudaGraphExec_t rexec = nullptr;
+            rc = chunk_graph(h, rem, false, &rexec);
+            if (rc != ISING_OK) return rc;
+            TRY_CUDA(cudaGraphLaunch(rexec, h->stream));
+            s0 = n_sweeps;
+        }
     }
     for (int64_t s = s0; s < n_sweeps; ++s) {
         const u32 t = (u32)(t0 + (uint64_t)s);

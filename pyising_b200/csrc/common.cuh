@@ -6,6 +6,8 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace ising {
@@ -158,6 +160,35 @@ inline u32 fast_div_magic(u32 d, unsigned long long n_max)
 {
     if (d < 2 || n_max * d >= (1ull << 32)) return 0;
     return (u32)(((1ull << 32) + d - 1) / d);
+}
+
+// Programmatic dependent launch.  Half-sweep kernels are launched with programmatic stream
+// serialization (launch_pdl), so a half-sweep's grid may be launched while the previous kernel
+// of the stream is still running: hiding the launch latency, which for small lattices is most
+// of a half-sweep.  Each such kernel waits in pdl_wait (griddepcontrol.wait: the previous grid
+// has completed and its writes are visible) before it reads the lattice or the control block,
+// then lets its own successor launch (pdl_trigger).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                              Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // Resolve the graph-replay control block of a launch (see Int8Half::ctl).

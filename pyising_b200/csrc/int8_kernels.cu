@@ -15,12 +15,14 @@ template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
 __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
 {
     Int8Half p = p_in;
-    resolve_ctl(p);
     __shared__ u32 stab[8];  // acceptance table for the per-site lookup rules
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) stab[i] = p.table[i];  // constant indices: p stays in registers
     }
+    pdl_wait();  // the previous half-sweep has completed
+    pdl_trigger();
+    resolve_ctl(p);
     __syncthreads();
     long long m_acc = 0, e_acc = 0;
     const u32 cpr = (u32)p.cpr, bpp = (u32)p.bpp;
@@ -46,17 +48,14 @@ template <int V, int NDIM, bool MIXED, bool MEAS>
 static cudaError_t launch_rule(int rule, const Int8Half& p, unsigned grid, cudaStream_t st)
 {
     switch (rule) {
-    case kMetroFast: int8_half_kernel<V, NDIM, kMetroFast, MIXED, MEAS><<<grid, 256, 0, st>>>(p); break;
-    case kHeatFast: int8_half_kernel<V, NDIM, kHeatFast, MIXED, MEAS><<<grid, 256, 0, st>>>(p); break;
+    case kMetroFast: return launch_pdl(int8_half_kernel<V, NDIM, kMetroFast, MIXED, MEAS>, grid, 256, st, p);
+    case kHeatFast: return launch_pdl(int8_half_kernel<V, NDIM, kHeatFast, MIXED, MEAS>, grid, 256, st, p);
     case kMetroGeneric:
-        int8_half_kernel<V, NDIM, kMetroGeneric, MIXED, MEAS><<<grid, 256, 0, st>>>(p);
-        break;
+        return launch_pdl(int8_half_kernel<V, NDIM, kMetroGeneric, MIXED, MEAS>, grid, 256, st, p);
     case kHeatGeneric:
-        int8_half_kernel<V, NDIM, kHeatGeneric, MIXED, MEAS><<<grid, 256, 0, st>>>(p);
-        break;
-    default: int8_half_kernel<V, NDIM, kObserve, MIXED, true><<<grid, 256, 0, st>>>(p); break;
+        return launch_pdl(int8_half_kernel<V, NDIM, kHeatGeneric, MIXED, MEAS>, grid, 256, st, p);
+    default: return launch_pdl(int8_half_kernel<V, NDIM, kObserve, MIXED, true>, grid, 256, st, p);
     }
-    return cudaGetLastError();
 }
 
 template <int V, bool MIXED = false>

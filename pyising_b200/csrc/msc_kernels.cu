@@ -33,10 +33,12 @@ __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
     msc_half_queue_kernel(const MscHalf p_in, long long total, long long per_warp, int nw_shift)
 {
     MscHalf p = p_in;
-    resolve_ctl(p);
     __shared__ QueueSlots q_all[kQueueWarps];
     __shared__ uint4 lvmask[16];
     if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+    pdl_wait();  // the previous half-sweep has completed
+    pdl_trigger();
+    resolve_ctl(p);
     __syncthreads();
     const long long begin = ((long long)blockIdx.x * kQueueWarps + (threadIdx.x >> 5)) * per_warp;
     const long long end = min(begin + per_warp, total);
@@ -101,9 +103,8 @@ cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int s
         if (per_warp < 32) per_warp = 32;
         const long long nwarps = (total + per_warp - 1) / per_warp;
         const unsigned blocks = (unsigned)((nwarps + kQueueWarps - 1) / kQueueWarps);
-        msc_half_queue_kernel<<<blocks, kQueueWarps * 32, 0, st>>>(p, total, per_warp,
-                                                                   msc_nw_shift(p.nw));
-        return cudaGetLastError();
+        return launch_pdl(msc_half_queue_kernel, dim3(blocks), dim3(kQueueWarps * 32), st, p,
+                          total, per_warp, msc_nw_shift(p.nw));
     }
     dim3 grid, block;
     msc_geometry(p.rows, p.nw, max_blocks, &grid, &block);
