@@ -1,10 +1,12 @@
 """Run one small sweep case, for profilers (ncu) and quick timing.
 
-    python -m pyising_b200.profile_case {int8|hb3|msc} L SWEEPS
+    python -m pyising_b200.profile_case {int8|hb3|msc|batch} L SWEEPS
 
 int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
-beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7.
-Prints the final exact (M, E).
+beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7;
+batch: an ensemble of 2D int8 Metropolis lattices L x L, L/2 x L/2 (four each) and L/4 x L/4
+(sixteen) at temperatures 2.0 .. 2.6, device seeded starts, SWEEPS sweeps with (M, E) every 10,
+through the batched kernel.  Prints the final exact (M, E) (batch: of the first lattice).
 """
 
 from __future__ import annotations
@@ -23,6 +25,18 @@ def main(argv: list[str]) -> int:
         sim = B200Int8((L, L, L), 0.221654626, seed=0, algorithm="heatbath", init="cold")
     elif which == "msc":
         sim = B200MultiSpin((L, L), BETA_C_2D, seed=7, init="hot")
+    elif which == "batch":
+        from .ensemble import Ensemble, Job
+
+        sizes = [L] + [L // 2] * 4 + [L // 4] * 16
+        jobs = [Job((s, s), 1.0 / (2.0 + 0.6 * i / len(sizes)), n, seed=i, measure_every=10,
+                    init="philox") for i, s in enumerate(sizes)]
+        with Ensemble() as ens:
+            ids = [ens.add(j) for j in jobs]
+            ens.run()
+            series = ens.result(ids[0]).series
+        print(which, L, n, tuple(int(x) for x in series[-1]) if len(series) else None)
+        return 0
     else:
         raise SystemExit(f"unknown case {which!r}")
     sim.sweep(n)

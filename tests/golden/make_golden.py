@@ -18,6 +18,8 @@ Files written (all ``.npz``):
   c2_msc.npz          msc 1024^2 x 1000 sweeps and 2048^2 x 200 sweeps, T_c, seed 7, hot.
   c3_int8_3d_L64.npz  64^3 int8 heat bath, beta 0.221654626, cold, 2000 sweeps, (M, E) every 10.
   c4_batch.npz        the first lattices (L <= 128) of the seeded 96-lattice ensemble, 500 sweeps.
+  exact.npz       pyising.exact: energy_torus / specific_heat_torus on a (T, L) grid,
+                  magnetization_2d and energy_2d on a T grid (``--only exact`` writes just this).
 Lattices are stored as np.packbits(lat > 0) with their shape.
 """
 
@@ -70,13 +72,29 @@ def kat_vectors(ref_root: Path):
     raise RuntimeError("KAT list not found")
 
 
+def write_exact() -> None:
+    """The reference's exact finite-torus and infinite-lattice results (src/pyising/exact.py)."""
+    from pyising import exact
+
+    Ts = np.array([1.5, 1.8, 2.0, 2.2, exact.TC_2D, 2.4, 2.6, 3.0, 4.0])
+    Ls = np.array([4, 8, 16, 32, 64, 128])
+    e = np.array([[exact.energy_torus(float(T), int(L)) for L in Ls] for T in Ts])
+    c = np.array([[exact.specific_heat_torus(float(T), int(L)) for L in Ls] for T in Ts])
+    np.savez_compressed(OUT / "exact.npz", T=Ts, L=Ls, energy_torus=e, specific_heat_torus=c,
+                        magnetization_2d=exact.magnetization_2d(Ts), energy_2d=exact.energy_2d(Ts))
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/src")
     ap.add_argument("--quick", action="store_true", help="skip the long config runs")
+    ap.add_argument("--only", choices=["exact"], default=None, help="write one fixture only")
     args = ap.parse_args()
     ref_root = Path(args.reference)
     sys.path.insert(0, str(ref_root))
+    write_exact()
+    if args.only == "exact":
+        return 0
     from pyising import backends as B
     from pyising.exact import BETA_C_2D
     from pyising.lattice import random_lattice, threshold_table
