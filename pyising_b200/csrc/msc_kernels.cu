@@ -29,6 +29,7 @@ __global__ void __launch_bounds__(256) msc_half_kernel(const MscHalf p_in)
 
 constexpr int kQueueWarps = 8;
 
+template <bool MEAS>
 __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
     msc_half_queue_kernel(const MscHalf p_in, long long total, long long per_warp, int nw_shift)
 {
@@ -43,7 +44,7 @@ __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
     const long long begin = ((long long)blockIdx.x * kQueueWarps + (threadIdx.x >> 5)) * per_warp;
     const long long end = min(begin + per_warp, total);
     msc_queue_range(p, begin, end, nw_shift, q_all[threadIdx.x >> 5], lvmask);
-    if (p.meas) {
+    if constexpr (MEAS) {
         // the warp's words are final: measure them (the other colour is unchanged)
         __syncwarp();
         long long m_acc = 0, e_acc = 0;
@@ -76,7 +77,7 @@ static int queue_blocks_per_sm()
     if (dev < 0 || dev >= 64) dev = 0;
     if (!cached[dev]) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_half_queue_kernel,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_half_queue_kernel<false>,
                                                           kQueueWarps * 32, 0) != cudaSuccess ||
             b < 1) {
             cudaGetLastError();
@@ -103,8 +104,11 @@ cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int s
         if (per_warp < 32) per_warp = 32;
         const long long nwarps = (total + per_warp - 1) / per_warp;
         const unsigned blocks = (unsigned)((nwarps + kQueueWarps - 1) / kQueueWarps);
-        return launch_pdl(msc_half_queue_kernel, dim3(blocks), dim3(kQueueWarps * 32), st, p,
-                          total, per_warp, msc_nw_shift(p.nw));
+        if (p.meas)
+            return launch_pdl(msc_half_queue_kernel<true>, dim3(blocks), dim3(kQueueWarps * 32),
+                              st, p, total, per_warp, msc_nw_shift(p.nw));
+        return launch_pdl(msc_half_queue_kernel<false>, dim3(blocks), dim3(kQueueWarps * 32), st,
+                          p, total, per_warp, msc_nw_shift(p.nw));
     }
     dim3 grid, block;
     msc_geometry(p.rows, p.nw, max_blocks, &grid, &block);
