@@ -256,7 +256,17 @@ def run_e2e(wl: str, steps: int, rank: int, world: int, dist, tuned: dict | None
     if tuned:
         autotune.apply(sim, tuned["config"])
     st0 = sim.state()
-    c0, c1 = st0["c0"], st0["c1"]
+
+    def pinned_like(a: np.ndarray) -> np.ndarray:
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        return t.numpy().view(a.dtype).reshape(a.shape)
+
+    # the step's input and result live in pinned host buffers (allocated once, outside the
+    # timed region), as a serving caller would keep them
+    c0, c1 = pinned_like(st0["c0"]), pinned_like(st0["c1"])
+    c0[...] = st0["c0"]
+    c1[...] = st0["c1"]
+    out = (pinned_like(st0["c0"]), pinned_like(st0["c1"]))
     h2d = c0.nbytes + c1.nbytes + sim.table.nbytes
     d2h = c0.nbytes + c1.nbytes + 16 + (sweeps // every) * 16 if every else c0.nbytes + c1.nbytes + 16
     sim.sweep(2)
@@ -264,6 +274,7 @@ def run_e2e(wl: str, steps: int, rank: int, world: int, dist, tuned: dict | None
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    finals = []
     t0 = time.perf_counter()
     for _ in range(steps):
         sim.load_colour_arrays(c0, c1)
@@ -273,8 +284,8 @@ def run_e2e(wl: str, steps: int, rank: int, world: int, dist, tuned: dict | None
             sim.sweep_measured(sweeps, every)
         else:
             sim.sweep(sweeps)
-        sim.colour_arrays()
-        sim.observables_int()
+        sim.colour_arrays(out)
+        finals.append(sim.observables_int())
     sim.synchronize()
     dt = time.perf_counter() - t0
     if dist is not None:
@@ -284,7 +295,9 @@ def run_e2e(wl: str, steps: int, rank: int, world: int, dist, tuned: dict | None
     n = int(np.prod(shape))
     return {"value": n * sweeps * steps * world / (dt * 1e9), "unit": "flips/ns",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": dt * 1e3 / steps}
+            "ms_per_step": dt * 1e3 / steps, "host_buffers": "pinned",
+            # every step runs the same job from the same start: identical (M, E) each time
+            "steps_identical": all(f == finals[0] for f in finals)}
 
 
 def rng_ceiling(sim, variant: str) -> dict:

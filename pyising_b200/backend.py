@@ -142,17 +142,39 @@ class _B200Simulation(IsingSimulation):
         check(lib().ising_set_stream(self._h, stream or None), "set_stream")
 
     # ---- checkpoint / resume -----------------------------------------------------------------
-    def colour_arrays(self) -> tuple[np.ndarray, np.ndarray]:
-        """The two colour arrays in their device layout (compressed int8 or packed uint64)."""
-        a, b = self._colour_buffers()
+    def colour_arrays(self, out: tuple[np.ndarray, np.ndarray] | None = None
+                      ) -> tuple[np.ndarray, np.ndarray]:
+        """The two colour arrays in their device layout (compressed int8 or packed uint64).
+        ``out``: two C-contiguous arrays of that shape and dtype to fill (e.g. pinned host
+        buffers reused across calls); new arrays otherwise."""
+        if out is None:
+            a, b = self._colour_buffers()
+        else:
+            a, b = (self._checked_buffer(x) for x in out)
         check(lib().ising_download(self._h, a.ctypes.data, b.ctypes.data), "download")
         return a, b
 
     def load_colour_arrays(self, c0: np.ndarray, c1: np.ndarray) -> None:
-        a, b = self._colour_buffers()
-        a[...] = c0
-        b[...] = c1
-        check(lib().ising_upload(self._h, a.ctypes.data, b.ctypes.data), "upload")
+        """Uploads two colour arrays in the device layout; C-contiguous arrays of the right
+        shape and dtype are read in place (no host copy)."""
+        shape, dtype = self._colour_spec()
+        src = []
+        for x in (c0, c1):
+            x = np.asarray(x)
+            if x.dtype != dtype or x.shape != shape or not x.flags.c_contiguous:
+                x = np.ascontiguousarray(x, dtype=dtype).reshape(shape)
+            src.append(x)
+        check(lib().ising_upload(self._h, src[0].ctypes.data, src[1].ctypes.data), "upload")
+
+    def _colour_buffers(self):
+        shape, dtype = self._colour_spec()
+        return np.empty(shape, dtype), np.empty(shape, dtype)
+
+    def _checked_buffer(self, x: np.ndarray) -> np.ndarray:
+        shape, dtype = self._colour_spec()
+        if x.dtype != dtype or x.shape != shape or not x.flags.c_contiguous:
+            raise ValueError(f"colour buffer must be C-contiguous {dtype} of shape {shape}")
+        return x
 
     def state(self) -> dict:
         """Everything needed to resume bit-exactly: the RNG is keyed by (site, t, colour, seed)."""
@@ -176,8 +198,8 @@ class B200Int8(_B200Simulation):
     stream = "int8"
     _variant_code = 0
 
-    def _colour_buffers(self):
-        return (np.empty((self.rows, self.lh), np.int8), np.empty((self.rows, self.lh), np.int8))
+    def _colour_spec(self):
+        return (self.rows, self.lh), np.dtype(np.int8)
 
 
 class B200MultiSpin(_B200Simulation):
@@ -191,9 +213,8 @@ class B200MultiSpin(_B200Simulation):
     bytes_per_update = 3.0 / 8.0
     _variant_code = 1
 
-    def _colour_buffers(self):
-        nw = self.lh // 64
-        return (np.empty((self.rows, nw), np.uint64), np.empty((self.rows, nw), np.uint64))
+    def _colour_spec(self):
+        return (self.rows, self.lh // 64), np.dtype(np.uint64)
 
     def philox_calls_per_word(self, sweeps: int = 2, warp: bool = False) -> float:
         """Mean (or per-warp maximum) Philox calls per word; advances the lattice like

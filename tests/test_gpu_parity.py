@@ -242,6 +242,29 @@ def test_checkpoint_resume_is_bit_exact(B, oracle_mod):
         np.testing.assert_array_equal(a.get_lattice(), b.get_lattice())
 
 
+def test_colour_arrays_into_caller_buffers(B, oracle_mod):
+    shape = (24, 1032)  # int8 rows padded on the device: host rows stay 516 bytes
+    for cls, sh in ((B.B200Int8, shape), (B.B200MultiSpin, (32, 256))):
+        lat = oracle_mod.random_lattice(sh, 9)
+        sim = cls(sh, 0.4, seed=3, init=lat)
+        sim.sweep(5)
+        want = sim.colour_arrays()
+        out = (np.empty_like(want[0]), np.empty_like(want[1]))
+        got = sim.colour_arrays(out)
+        assert got[0] is out[0] and got[1] is out[1]
+        np.testing.assert_array_equal(out[0], want[0])
+        np.testing.assert_array_equal(out[1], want[1])
+        with pytest.raises(ValueError):
+            sim.colour_arrays((out[0][:, :-1].copy(), out[1]))
+        # in-place upload of contiguous arrays, and of strided ones (copied)
+        sim.load_colour_arrays(out[0], out[1])
+        np.testing.assert_array_equal(sim.colour_arrays()[0], want[0])
+        wide = np.zeros((want[1].shape[0], 2 * want[1].shape[1]), want[1].dtype)
+        wide[:, ::2] = want[1]
+        sim.load_colour_arrays(want[0], wide[:, ::2])
+        np.testing.assert_array_equal(sim.colour_arrays()[1], want[1])
+
+
 def test_msc_calls_per_word_diagnostic(B, oracle_mod):
     shape = (256, 1024)
     lat = oracle_mod.random_lattice(shape, 1)
