@@ -412,7 +412,7 @@ def run_batched_ensemble() -> dict:
 
     jobs = c4_jobs()
     flips = sum(j.n_spins * j.sweeps for j in jobs)
-    tuned = autotune.tune_ensemble(jobs, sweeps=100)
+    tuned = autotune.tune_ensemble(jobs, sweeps=256)
     with Ensemble(memory_budget=120e9) as ens:
         for name, v in tuned["config"].items():
             ens.set_knob(name, v)
@@ -447,7 +447,7 @@ def run_served_stream(n_jobs: int) -> dict:
     flips = sum(j.n_spins * j.sweeps for j in jobs)
     submit_t = [0.0] * n_jobs
     ids = [0] * n_jobs
-    tuned = autotune.tune_ensemble(jobs[: min(n_jobs, 100)], sweeps=100)
+    tuned = autotune.tune_ensemble(jobs[: min(n_jobs, 100)], sweeps=256)
     with Server(memory_budget=120e9) as srv:
         for name, v in tuned["config"].items():
             srv.set_knob(name, v)

@@ -142,7 +142,8 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
 /* Batch and server knobs (ising_batch_set_knob, ising_server_set_knob): ISING_KNOB_BAND is the
  * longest band a kernel class may use (default 8); ISING_KNOB_ITEMS_PER_SLOT the work items per
  * resident block a launch aims at (default 6; smaller items balance better, larger ones cost
- * less per item). */
+ * less per item); ISING_KNOB_GRAPH_CHUNK the sweeps of a stable batch replayed from one
+ * captured graph (default 32, 0 = every epoch launched directly). */
 #define ISING_KNOB_ITEMS_PER_SLOT 6
 int ising_set_knob(ising_sim* h, int knob, int value);
 int ising_get_knob(ising_sim* h, int knob, int* value);

@@ -230,12 +230,13 @@ def tune(variant: str, shape, algorithm: str = "metropolis", beta: float | None 
     return result
 
 
-BATCH_SPACE = {"band": [8, 4, 2, 16], "items_per_slot": [6, 3, 12]}
+BATCH_SPACE = {"band": [8, 4, 2, 16], "items_per_slot": [6, 3, 12], "graph_chunk": [32, 8, 0]}
 
 
 def tune_ensemble(jobs, sweeps: int = 200, device: int = 0) -> dict:
-    """Coordinate descent over the batch knobs (:data:`BATCH_SPACE`) on copies of ``jobs``
-    shortened to ``sweeps`` sweeps (same shapes, variants and temperatures, so the same kernel
+    """Coordinate descent over the batch knobs (:data:`BATCH_SPACE`: band cap, items per
+    resident block, sweeps per replayed graph chunk) on copies of ``jobs`` shortened to
+    ``sweeps`` sweeps (same shapes, variants and temperatures, so the same kernel
     classes and work lists); returns ``{"config": ..., "flips_per_ns": ..., "trials": ...}``."""
     import dataclasses
 

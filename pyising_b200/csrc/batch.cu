@@ -14,6 +14,7 @@
 // so it never waits for the device except to hand results back (events) and to bound how far
 // it runs ahead.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -85,7 +86,8 @@ constexpr int kInt8PerLaunch = 240;
 
 template <int N>
 struct Int8LaunchN {
-    long long epoch;
+    long long epoch;               // the launch's epoch, relative to *epoch_base when set
+    const long long* epoch_base;   // replayed graph chunks: device epoch counter, else nullptr
     int n;  // lattices
     int pad;
     Int8Desc lat[N];
@@ -141,8 +143,9 @@ __global__ void __launch_bounds__(256, ISING_BATCH_MIN_BLOCKS)
         }
         __syncthreads();
     }
-    const u32 color = (u32)(P.epoch & 1);
-    const u32 s = (u32)((P.epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
+    const long long epoch = P.epoch + (P.epoch_base ? *P.epoch_base : 0);
+    const u32 color = (u32)(epoch & 1);
+    const u32 s = (u32)((epoch - L.join_epoch) >> 1);  // sweeps done (< 2^31)
     const bool meas = color == 1 && L.every > 0 && ((s + 1u) % (u32)L.every) == 0;
     Int8Half p;
     p.own = static_cast<int8_t*>(L.c[color]);
@@ -186,12 +189,14 @@ constexpr int kBatchWarps = 8;
 
 __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
     const BatchLattice* __restrict__ lats, const BatchItem* __restrict__ items, int n_items,
-    long long epoch)
+    long long epoch_rel, const long long* epoch_base)
 {
     __shared__ QueueSlots q_all[kBatchWarps];
     __shared__ uint4 lvmask[16];
     // (launched without programmatic serialization: its early-launched blocks would hold their
     // 17 KB work stacks while waiting, and the batch measured slower with it)
+    // the epoch, relative to the device counter in replayed graph chunks
+    const long long epoch = epoch_rel + (epoch_base ? *epoch_base : 0);
     const u32 color = (u32)(epoch & 1);
     const int warp = threadIdx.x >> 5;
     long long m_acc = 0, e_acc = 0;  // flushed per lattice, as in batch_int8_kernel
@@ -237,6 +242,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32) batch_msc_kernel(
         __syncthreads();
     }
 }
+
+__global__ void batch_epoch_set(long long* counter, long long epoch) { *counter = epoch; }
 
 // ----------------------------------------------------------------------------- host engine ---
 
@@ -293,6 +300,8 @@ public:
         uint64_t keep = (uint64_t)budget_;
         e = cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolSetAttribute");
+        e = cudaMalloc((void**)&d_epoch_, sizeof(long long));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (epoch counter)");
         return ISING_OK;
     }
 
@@ -304,6 +313,12 @@ public:
         if (d_lats_) cudaFreeAsync(d_lats_, stream_);
         if (d_items_) cudaFreeAsync(d_items_, stream_);
         if (stream_) cudaStreamSynchronize(stream_);
+        if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
+        for (auto& x : old_execs_) {
+            cudaGraphExecDestroy(x.first);
+            cudaEventDestroy(x.second);
+        }
+        if (d_epoch_) cudaFree(d_epoch_);
         for (auto& kv : pinned_free_) cudaFreeHost(kv.second);
         for (cudaEvent_t ev : epoch_events_) cudaEventDestroy(ev);
         if (stream_) cudaStreamDestroy(stream_);
@@ -352,20 +367,19 @@ public:
         }
         if (active_.empty()) return ISING_OK;
         if (dirty_) {
+            drop_chunk();
             int rc = rebuild();
             if (rc != ISING_OK) return rc;
         }
-        for (auto& cl : int8_launches_) {
-            for (Int8Launch& P : cl.second) {
-                P.epoch = epoch_;
-                e = launch_int8(cl.first, P);
-                if (e != cudaSuccess) return cuda_fail(e, "batch launch (int8)");
-            }
+        reap_chunks();
+        if (chunk_ready()) {
+            int rc = run_chunk();
+            if (rc == ISING_OK) rc = retire();
+            if (rc == ISING_OK) rc = throttle();
+            return rc;
         }
-        for (const auto& cl : classes_) {
-            e = launch_msc(cl.second.first, cl.second.second);
-            if (e != cudaSuccess) return cuda_fail(e, "batch launch (msc)");
-        }
+        e = launch_epoch(epoch_, nullptr);
+        if (e != cudaSuccess) return cuda_fail(e, "batch launch");
         ++epoch_;
         if ((epoch_ & 1) == 0) {
             int rc = retire();
@@ -460,6 +474,11 @@ public:
             if (value < 1 || value > 64)
                 return fail(ISING_ERR_INVALID, "items per slot must be 1..64");
             items_per_slot_ = value;
+        } else if (knob == ISING_KNOB_GRAPH_CHUNK) {
+            if (value < 0 || value > 64)
+                return fail(ISING_ERR_INVALID, "batch graph chunk must be 0..64 sweeps");
+            chunk_sweeps_ = value;
+            drop_chunk();
         } else {
             return fail(ISING_ERR_INVALID, "knob %d does not apply to a batch", knob);
         }
@@ -471,6 +490,7 @@ public:
     {
         if (knob == ISING_KNOB_BAND) *value = band_cap_;
         else if (knob == ISING_KNOB_ITEMS_PER_SLOT) *value = (int)items_per_slot_;
+        else if (knob == ISING_KNOB_GRAPH_CHUNK) *value = (int)chunk_sweeps_;
         else return fail(ISING_ERR_INVALID, "knob %d does not apply to a batch", knob);
         return ISING_OK;
     }
@@ -767,6 +787,7 @@ private:
     {
         Int8LaunchN<N> P;
         P.epoch = full.epoch;
+        P.epoch_base = full.epoch_base;
         P.n = full.n;
         P.pad = 0;
         memcpy(P.lat, full.lat, (size_t)full.n * sizeof(Int8Desc));
@@ -805,12 +826,115 @@ private:
                         : launch_int8_rule<16, 2, false>(kc.rule, P);
     }
 
-    cudaError_t launch_msc(int off, int n)
+    cudaError_t launch_msc(int off, int n, long long epoch, const long long* epoch_base)
     {
         auto fn = batch_msc_kernel;
         const dim3 grid(grid_for((const void*)fn, n, kBatchWarps * 32)), block(kBatchWarps * 32);
-        fn<<<grid, block, 0, stream_>>>(d_lats_, d_items_ + off, n, epoch_);
+        fn<<<grid, block, 0, stream_>>>(d_lats_, d_items_ + off, n, epoch, epoch_base);
         return cudaGetLastError();
+    }
+
+    // Every class's launches of one epoch (absolute, or relative to *epoch_base).
+    cudaError_t launch_epoch(long long epoch, const long long* epoch_base)
+    {
+        cudaError_t e = cudaSuccess;
+        for (auto& cl : int8_launches_) {
+            for (Int8Launch& P : cl.second) {
+                P.epoch = epoch;
+                P.epoch_base = epoch_base;
+                e = launch_int8(cl.first, P);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        for (const auto& cl : classes_) {
+            e = launch_msc(cl.second.first, cl.second.second, epoch, epoch_base);
+            if (e != cudaSuccess) return e;
+        }
+        return e;
+    }
+
+    // ---- graph chunks: kChunkSweeps sweeps of a stable batch replayed from one graph ----
+    // While no job can join (admission happens at even epochs, and pending jobs that did not
+    // fit can only fit after a job retires) and every active job has kChunkSweeps sweeps left,
+    // the batch's launches repeat with only the epoch changing: they are captured once per
+    // membership, reading the epoch from a device counter set before each replay.
+    static constexpr long long kChunkSweeps = 32;  // default of the ISING_KNOB_GRAPH_CHUNK knob
+    static constexpr long long kChunkReplays = 4;  // chunks of sweeps left needed for a capture
+
+    long long min_sweeps_left() const
+    {
+        long long m = LLONG_MAX;
+        for (int64_t id : active_) {
+            const Job& j = *jobs_.at(id);
+            m = std::min(m, (long long)j.spec.n_sweeps - (epoch_ - j.join_epoch) / 2);
+        }
+        return m;
+    }
+
+    bool chunk_ready() const
+    {
+        if ((epoch_ & 1) || active_.empty() || chunk_sweeps_ == 0) return false;
+        return min_sweeps_left() >= chunk_sweeps_ * (chunk_exec_ ? 1 : kChunkReplays);
+    }
+
+    int run_chunk()
+    {
+        cudaError_t e;
+        if (!chunk_exec_) {
+            e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture (batch)");
+            cudaError_t le = cudaSuccess;
+            for (long long k = 0; k < 2 * chunk_sweeps_ && le == cudaSuccess; ++k)
+                le = launch_epoch(k, d_epoch_);
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(stream_, &graph);
+            if (le != cudaSuccess || e != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                return cuda_fail(le != cudaSuccess ? le : e, "batch graph capture");
+            }
+            e = cudaGraphInstantiate(&chunk_exec_, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                chunk_exec_ = nullptr;
+                return cuda_fail(e, "cudaGraphInstantiate (batch)");
+            }
+        }
+        batch_epoch_set<<<1, 1, 0, stream_>>>(d_epoch_, epoch_);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGraphLaunch(chunk_exec_, stream_);
+        if (e != cudaSuccess) return cuda_fail(e, "batch graph launch");
+        epoch_ += 2 * chunk_sweeps_;
+        return ISING_OK;
+    }
+
+    // Drops the chunk graph (membership changed); it is destroyed once its launches are done.
+    void drop_chunk()
+    {
+        if (!chunk_exec_) return;
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventRecord(ev, stream_) == cudaSuccess) {
+            old_execs_.emplace_back(chunk_exec_, ev);
+        } else {
+            cudaStreamSynchronize(stream_);
+            cudaGraphExecDestroy(chunk_exec_);
+            if (ev) cudaEventDestroy(ev);
+        }
+        chunk_exec_ = nullptr;
+    }
+
+    void reap_chunks()
+    {
+        for (auto it = old_execs_.begin(); it != old_execs_.end();) {
+            if (cudaEventQuery(it->second) == cudaSuccess) {
+                cudaGraphExecDestroy(it->first);
+                cudaEventDestroy(it->second);
+                it = old_execs_.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        cudaGetLastError();  // cudaErrorNotReady from the queries
     }
 
     int retire()
@@ -873,9 +997,10 @@ private:
         return ISING_OK;
     }
 
-    // Records the end of the sweep just issued; the host stays at most kMaxAhead sweeps ahead
-    // of the device (see throttle_event), so a newly admitted job starts soon after it joins.
-    static constexpr size_t kMaxAhead = 8;
+    // Records the end of the sweep (or graph chunk) just issued; the host stays at most about
+    // kMaxAhead sweeps ahead of the device (see throttle_event), so a newly admitted job starts
+    // soon after it joins.
+    static constexpr long long kMaxAhead = 8;
 
     int throttle()
     {
@@ -889,7 +1014,7 @@ private:
             epoch_events_.push_back(ev);
         }
         cudaEventRecord(ev, stream_);
-        inflight_.push_back(ev);
+        inflight_.emplace_back(ev, epoch_);
         return ISING_OK;
     }
 
@@ -898,12 +1023,14 @@ public:
     // wait without holding any lock the submitters need, then call throttle_done().
     cudaEvent_t throttle_event() const
     {
-        return inflight_.size() > kMaxAhead ? inflight_.front() : nullptr;
+        return !inflight_.empty() && epoch_ - inflight_.front().second > 2 * kMaxAhead
+                   ? inflight_.front().first
+                   : nullptr;
     }
 
     void throttle_done()
     {
-        free_events_.push_back(inflight_.front());
+        free_events_.push_back(inflight_.front().first);
         inflight_.pop_front();
     }
 
@@ -973,6 +1100,10 @@ private:
     int64_t last_id_ = 0;
     int band_cap_ = kBandCap;
     long long items_per_slot_ = kItemsPerSlot;
+    long long* d_epoch_ = nullptr;       // device epoch counter of replayed graph chunks
+    cudaGraphExec_t chunk_exec_ = nullptr;
+    std::vector<std::pair<cudaGraphExec_t, cudaEvent_t>> old_execs_;
+    long long chunk_sweeps_ = kChunkSweeps;  // 0: no graph chunks
     std::map<int64_t, std::unique_ptr<Job>> jobs_;
     std::deque<int64_t> pending_;
     std::vector<int64_t> active_;
@@ -985,7 +1116,7 @@ private:
     std::vector<std::pair<KernelClass, std::vector<Int8Launch>>> int8_launches_;
     std::vector<cudaEvent_t> epoch_events_, free_events_;
     std::map<const void*, int> occupancy_;
-    std::deque<cudaEvent_t> inflight_;
+    std::deque<std::pair<cudaEvent_t, long long>> inflight_;  // (event, epoch recorded at)
 };
 
 }  // namespace ising

@@ -139,11 +139,12 @@ class Ensemble:
         self._jobs[jid.value] = job
         return int(jid.value)
 
-    BATCH_KNOBS = {"band": 1, "items_per_slot": 6}
+    BATCH_KNOBS = {"band": 1, "items_per_slot": 6, "graph_chunk": 5}
 
     def set_knob(self, name: str, value: int) -> None:
         """Batch launch knob (``"band"``: longest band of a kernel class, ``"items_per_slot"``:
-        work items per resident block); results are identical for every value."""
+        work items per resident block, ``"graph_chunk"``: sweeps replayed from one captured
+        graph while the batch is stable, 0 = none); results are identical for every value."""
         check(lib().ising_batch_set_knob(self._b, self.BATCH_KNOBS[name], int(value)),
               "batch_set_knob")
 

@@ -132,7 +132,8 @@ def test_batch_knobs_give_identical_results():
         cls = B200MultiSpin if j.variant == "msc" else B200Int8
         sim = cls(j.shape, j.beta, seed=j.seed, algorithm=j.algorithm, init="philox")
         solo.append(sim.sweep_measured(j.sweeps, j.measure_every))
-    for cfg in [{"band": 1}, {"band": 2, "items_per_slot": 1}, {"band": 16, "items_per_slot": 12}]:
+    for cfg in [{"band": 1, "graph_chunk": 0}, {"band": 2, "items_per_slot": 1},
+                {"band": 16, "items_per_slot": 12, "graph_chunk": 1}, {"graph_chunk": 4}]:
         with Ensemble() as ens:
             for name, v in cfg.items():
                 ens.set_knob(name, v)
