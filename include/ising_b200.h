@@ -153,6 +153,24 @@ int ising_get_knob(ising_sim* h, int knob, int* value);
  * autotuner; the sweeps are real (the lattice advances).  No counterpart in the reference. */
 int ising_time_sweeps(ising_sim* h, uint64_t t0, int64_t n_sweeps, float* ms);
 
+/* n_steps Swendsen-Wang cluster updates of an int8 lattice (2D/3D, fewer than 2^31 sites),
+ * steps step0 .. step0+n-1, random numbers keyed by `seed`: bonds between aligned neighbours
+ * are active when a Philox uniform is below p_bond (the integer threshold of
+ * p = 1 - exp(-2 beta)), the connected clusters are found on the device by a lock-free
+ * union-find, and each cluster flips with probability 1/2.  Labels take 4 bytes per site,
+ * allocated on the first call.  ISING_ERR_TIMEOUT if a bounded union-find loop gave up.
+ * Replaces: the CPU Wolff sampler used for equilibrated starts and Binder scans
+ * (src/pyising/cluster.py:32-104; src/pyising/validate.py:45-50,127-150). */
+int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps, uint64_t seed,
+                        uint32_t p_bond);
+
+/* One labeling of step `step` without the flips (diagnostics and tests): labels_out (2*S
+ * int32, S = sites per colour; site g = c*S + row*Lx/2 + j) gets each site's cluster root,
+ * bonds_out (S bytes) the active bonds of each colour-0 site (bit k: same-index colour-1 site,
+ * the other horizontal one, y+1, y-1, z+1, z-1).  No counterpart in the reference. */
+int ising_cluster_labels(ising_sim* h, uint64_t step, uint64_t seed, uint32_t p_bond,
+                         int32_t* labels_out, uint8_t* bonds_out);
+
 /* Exact magnetisation M = sum s and energy E = -sum_<ij> s_i s_j (blocks until done).
  * Replaces: observables / magnetization / energy (src/pyising/backends/base.py:125-135;
  * src/pyising/backends/observables_torch.py:46-111). */

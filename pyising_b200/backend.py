@@ -11,6 +11,7 @@ seed and start.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 from typing import ClassVar
 
@@ -38,6 +39,7 @@ class _B200Simulation(IsingSimulation):
                                  _lib.ALGORITHM[self.algorithm], self.seed, self.device,
                                  ctypes.byref(self._h)), "create")
         self._upload_table()
+        self.cluster_t = 0
         # launch knobs picked by the autotuner for this GPU and shape, if any (speed only)
         from . import autotune
 
@@ -200,6 +202,38 @@ class B200Int8(_B200Simulation):
 
     def _colour_spec(self):
         return (self.rows, self.lh), np.dtype(np.int8)
+
+
+    # ---- cluster updates (Swendsen-Wang on the device) ------------------------------------
+    def bond_threshold(self) -> int:
+        """Integer threshold of the bond probability p = 1 - exp(-2 beta)."""
+        from .lattice import prob_to_threshold
+
+        return prob_to_threshold(1.0 - math.exp(-2.0 * self.beta)) if self.beta > 0 else 0
+
+    def cluster_sweep(self, n: int = 1, seed: int | None = None) -> None:
+        """``n`` Swendsen-Wang updates (steps ``self.cluster_t`` ..), keyed by ``seed`` (the
+        simulation's seed by default).  The Metropolis/heat-bath sweep counter ``t`` is not
+        touched; the cluster step counter ``cluster_t`` advances by ``n``."""
+        n = int(n)
+        if n <= 0:
+            return
+        key = self.seed if seed is None else int(seed) & 0xFFFFFFFFFFFFFFFF
+        check(lib().ising_cluster_sweep(self._h, self.cluster_t, n, key, self.bond_threshold()),
+              "cluster_sweep")
+        self.cluster_t += n
+
+    def cluster_labels(self, step: int = 0, seed: int | None = None) -> tuple[np.ndarray,
+                                                                              np.ndarray]:
+        """One Swendsen-Wang labeling without flips: (labels (2, rows, Lx/2) int32 = each
+        site's cluster root, bonds (rows, Lx/2) uint8 = active bonds of each colour-0 site)."""
+        key = self.seed if seed is None else int(seed) & 0xFFFFFFFFFFFFFFFF
+        labels = np.empty((2, self.rows, self.lh), np.int32)
+        bonds = np.empty((self.rows, self.lh), np.uint8)
+        check(lib().ising_cluster_labels(self._h, int(step), key, self.bond_threshold(),
+                                         labels.ctypes.data, bonds.ctypes.data),
+              "cluster_labels")
+        return labels, bonds
 
 
 class B200MultiSpin(_B200Simulation):

@@ -285,6 +285,7 @@ int ising_destroy(ising_sim* h)
     if (h->h_series) cudaFreeHost(h->h_series);
     clear_graphs(h);
     if (h->d_flags) cudaFree(h->d_flags);
+    if (h->d_label) cudaFree(h->d_label);
     if (h->own_stream_handle) cudaStreamDestroy(h->own_stream_handle);
     cudaGetLastError();
     delete h;

@@ -1,0 +1,262 @@
+// Swendsen-Wang cluster updates of an int8 lattice (2D/3D), in its checkerboard layout.
+//
+// Local updates slow down critically near T_c (autocorrelation ~ L^2.17 sweeps in 2D); pyising
+// equilibrates its starts and measures its Binder cumulants with a CPU Wolff sampler
+// (src/pyising/cluster.py:32-104, src/pyising/validate.py:45-50,127-150).  Here the cluster
+// update runs on the device: Swendsen-Wang (Phys. Rev. Lett. 58, 86 (1987)) with the
+// connected components found by a lock-free union-find.
+//
+// One update at step t:
+//   1. every site is its own tree: label[g] = g;
+//   2. every bond joins a colour-0 site to a colour-1 site (the lattice is bipartite), so each
+//      colour-0 site owns its 2d bonds and each bond is seen once.  A bond between aligned
+//      spins is active with probability p = 1 - exp(-2 beta) (threshold p_bond on a uniform
+//      u32 from Philox((n, t, kBondTag, k), key)); active bonds union their endpoints' trees:
+//      roots are linked larger-under-smaller with atomicCAS, finds halve paths with plain
+//      stores (parents only ever move up the tree, so a stale read is still an ancestor);
+//   3. every label is replaced by its root;
+//   4. every cluster flips with probability 1/2: bit (root & 127) of
+//      Philox((root >> 7, t, kFlipTag, 0), key), the same for all its sites.
+// Site g = c * S + row * lh + j (S = rows * lh sites per colour, the logical compressed index).
+// Labels are int32 (lattices of fewer than 2^31 sites).  Every retry loop is bounded: a thread
+// that exceeds the bound sets the error word and stops, and the host reports ISING_ERR_TIMEOUT.
+#include "capi_internal.h"
+
+namespace ising {
+
+constexpr u32 kBondTag = 0x53570001u;  // Philox counter word 2 of the bond uniforms
+constexpr u32 kFlipTag = 0x53570002u;  // ... of the cluster flip bits
+constexpr long long kFindLimit = 1ll << 24;
+constexpr long long kUnionLimit = 1ll << 20;
+
+struct ClusterArgs {
+    int8_t* c[2];
+    int* label;
+    unsigned char* bonds;  // per colour-0 site, bit k = bond k active (diagnostics), or nullptr
+    int* err;
+    long long S;           // sites per colour
+    long long rows;
+    int lh, ly, lz, pitch, ndim;
+    u32 t, k0, k1, p_bond;
+};
+
+__device__ __forceinline__ int uf_find(int* label, int x, int* err)
+{
+    for (long long it = 0; it < kFindLimit; ++it) {
+        const int p = __ldcg(label + x);
+        if (p == x) return x;
+        const int gp = __ldcg(label + p);
+        if (gp != p) label[x] = gp;  // path halving
+        x = gp;
+    }
+    atomicExch(err, 1);
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(int* label, int a, int b, int* err)
+{
+    for (long long it = 0; it < kUnionLimit; ++it) {
+        a = uf_find(label, a, err);
+        b = uf_find(label, b, err);
+        if (a == b) return;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        // link root b under root a, unless b stopped being a root meanwhile
+        const int old = atomicCAS(label + b, b, a);
+        if (old == b) return;
+        b = old;
+    }
+    atomicExch(err, 1);
+}
+
+__global__ void sw_init_kernel(int* label, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        label[i] = (int)i;
+}
+
+__global__ void sw_bond_kernel(const ClusterArgs a)
+{
+    const long long n0 = a.S;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < n0;
+         n += (long long)gridDim.x * blockDim.x) {
+        const long long row = n / a.lh;
+        const int j = (int)(n - row * a.lh);
+        const int y = (int)(row % a.ly), z = (int)(row / a.ly);
+        const int par = (y + z) & 1;  // colour 0
+        const int8_t s = a.c[0][row * a.pitch + j];
+        // the 2d colour-1 neighbours: same index, the other horizontal one, y -+ 1, z -+ 1
+        long long nb[6];
+        const long long plane = (long long)z * a.ly;
+        nb[0] = row * a.lh + j;
+        nb[1] = row * a.lh + (par ? (j + 1 == a.lh ? 0 : j + 1) : (j == 0 ? a.lh - 1 : j - 1));
+        nb[2] = (plane + (y + 1 == a.ly ? 0 : y + 1)) * a.lh + j;
+        nb[3] = (plane + (y == 0 ? a.ly - 1 : y - 1)) * a.lh + j;
+        nb[4] = ((long long)(z + 1 == a.lz ? 0 : z + 1) * a.ly + y) * a.lh + j;
+        nb[5] = ((long long)(z == 0 ? a.lz - 1 : z - 1) * a.ly + y) * a.lh + j;
+        const u32x4 r0 = philox4x32_10((u32)n, a.t, kBondTag, 0u, a.k0, a.k1);
+        u32x4 r1 = {0u, 0u, 0u, 0u};
+        if (a.ndim == 3) r1 = philox4x32_10((u32)n, a.t, kBondTag, 1u, a.k0, a.k1);
+        const u32 u[6] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y};
+        unsigned mask = 0;
+        const int nbonds = 2 * a.ndim;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            if (k >= nbonds) break;
+            const long long m = nb[k];
+            const long long mrow = m / a.lh;
+            const int8_t sn = a.c[1][mrow * a.pitch + (m - mrow * a.lh)];
+            if (sn == s && u[k] < a.p_bond) {
+                mask |= 1u << k;
+                uf_union(a.label, (int)n, (int)(n0 + m), a.err);
+            }
+        }
+        if (a.bonds) a.bonds[n] = (unsigned char)mask;
+    }
+}
+
+__global__ void sw_flatten_kernel(int* label, long long n, int* err)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        label[i] = uf_find(label, (int)i, err);
+}
+
+__global__ void sw_flip_kernel(const ClusterArgs a)
+{
+    const long long n = 2 * a.S;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int root = a.label[g];
+        const u32x4 r = philox4x32_10((u32)root >> 7, a.t, kFlipTag, 0u, a.k0, a.k1);
+        const u32 w = (root & 64) ? ((root & 32) ? r.w : r.z) : ((root & 32) ? r.y : r.x);
+        if ((w >> (root & 31)) & 1u) {
+            const int c = g >= a.S ? 1 : 0;
+            const long long m = g - (long long)c * a.S;
+            const long long row = m / a.lh;
+            int8_t* p = a.c[c] + row * a.pitch + (m - row * a.lh);
+            *p = (int8_t)(*p ^ (int8_t)0xFE);  // +1 <-> -1
+        }
+    }
+}
+
+static int cluster_setup(ising_sim* h)
+{
+    if (h->variant != ISING_VARIANT_INT8)
+        return fail(ISING_ERR_INVALID, "cluster updates: int8 lattices only");
+    const long long n = 2 * h->rows * (long long)h->lh;
+    if (n >= 0x7FFFFFFFll)
+        return fail(ISING_ERR_INVALID, "cluster updates: lattices of fewer than 2^31 sites");
+    if (!h->d_label) {
+        cudaError_t e = cudaMalloc((void**)&h->d_label, (size_t)n * sizeof(int) + 256);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ISING_ERR_NOMEM, "cudaMalloc of the cluster labels (%lld sites)", n);
+        }
+    }
+    return ISING_OK;
+}
+
+// One labeling (steps 1-3) and, when `flip`, the cluster flips (step 4).
+static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip,
+                        unsigned char* bonds)
+{
+    ClusterArgs a;
+    a.c[0] = (int8_t*)h->c[0];
+    a.c[1] = (int8_t*)h->c[1];
+    a.S = h->rows * (long long)h->lh;
+    a.label = h->d_label;
+    a.err = reinterpret_cast<int*>(reinterpret_cast<char*>(h->d_label) + 2 * a.S * sizeof(int));
+    a.bonds = bonds;
+    a.rows = h->rows;
+    a.lh = h->lh;
+    a.ly = h->ly;
+    a.lz = h->lz;
+    a.pitch = h->pitch;
+    a.ndim = h->ndim;
+    a.t = t;
+    a.k0 = (u32)seed;
+    a.k1 = (u32)(seed >> 32);
+    a.p_bond = p_bond;
+    const int grid = h->sm_count * 8;
+    sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
+    sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);
+    sw_flatten_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S, a.err);
+    if (flip) sw_flip_kernel<<<grid, 256, 0, h->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "cluster update launch");
+    return ISING_OK;
+}
+
+static int cluster_error(ising_sim* h)
+{
+    const long long S = h->rows * (long long)h->lh;
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, reinterpret_cast<char*>(h->d_label) + 2 * S * sizeof(int),
+                                    sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cluster update");
+    if (err) return fail(ISING_ERR_TIMEOUT, "a bounded union-find loop of the cluster update gave up");
+    return ISING_OK;
+}
+
+}  // namespace ising
+
+using namespace ising;
+
+extern "C" int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps, uint64_t seed,
+                                   uint32_t p_bond)
+{
+    if (!h) return fail(ISING_ERR_INVALID, "null handle");
+    if (n_steps < 0) return fail(ISING_ERR_INVALID, "negative step count");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    int rc = cluster_setup(h);
+    if (rc != ISING_OK) return rc;
+    const long long S = h->rows * (long long)h->lh;
+    e = cudaMemsetAsync(reinterpret_cast<char*>(h->d_label) + 2 * S * sizeof(int), 0, sizeof(int),
+                        h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    for (int64_t k = 0; k < n_steps; ++k) {
+        rc = cluster_step(h, (u32)(step0 + (uint64_t)k), seed, p_bond, true, nullptr);
+        if (rc != ISING_OK) return rc;
+    }
+    return cluster_error(h);
+}
+
+extern "C" int ising_cluster_labels(ising_sim* h, uint64_t step, uint64_t seed, uint32_t p_bond,
+                                    int32_t* labels_out, uint8_t* bonds_out)
+{
+    if (!h || !labels_out || !bonds_out) return fail(ISING_ERR_INVALID, "null argument");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    int rc = cluster_setup(h);
+    if (rc != ISING_OK) return rc;
+    const long long S = h->rows * (long long)h->lh;
+    unsigned char* d_bonds = nullptr;
+    e = cudaMalloc((void**)&d_bonds, (size_t)S);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (bonds)");
+    e = cudaMemsetAsync(reinterpret_cast<char*>(h->d_label) + 2 * S * sizeof(int), 0, sizeof(int),
+                        h->stream);
+    if (e == cudaSuccess) {
+        rc = cluster_step(h, (u32)step, seed, p_bond, false, d_bonds);
+        if (rc == ISING_OK) rc = cluster_error(h);
+        if (rc == ISING_OK) {
+            e = cudaMemcpyAsync(labels_out, h->d_label, (size_t)(2 * S) * sizeof(int),
+                                cudaMemcpyDeviceToHost, h->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(bonds_out, d_bonds, (size_t)S, cudaMemcpyDeviceToHost,
+                                    h->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+            if (e != cudaSuccess) rc = cuda_fail(e, "cluster labels copy");
+        }
+    } else {
+        rc = cuda_fail(e, "cudaMemsetAsync");
+    }
+    cudaFree(d_bonds);
+    return rc;
+}

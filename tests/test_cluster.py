@@ -1,0 +1,111 @@
+"""Swendsen-Wang cluster updates on the device (ising_cluster_sweep / ising_cluster_labels).
+
+There is no bit-exact reference for them (pyising's own cluster sampler is a CPU Wolff with
+NumPy's generator, src/pyising/cluster.py:32-104), so the labeling is checked exactly against a
+CPU union-find over the same active bonds, the bond rule against the spins, and the dynamics
+statistically against the exact finite-torus energy (host FP64, pyising_b200.physics).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def neighbours(shape, c0_row, j):
+    """Colour-1 neighbours of colour-0 site (row, j) in the order of the bond bits."""
+    ndim = len(shape)
+    lh = shape[-1] // 2
+    ly = shape[-2]
+    lz = shape[0] if ndim == 3 else 1
+    y, z = c0_row % ly, c0_row // ly
+    par = (y + z) & 1
+    plane = z * ly
+    out = [c0_row * lh + j,
+           c0_row * lh + ((j + 1) % lh if par else (j - 1) % lh),
+           (plane + (y + 1) % ly) * lh + j,
+           (plane + (y - 1) % ly) * lh + j]
+    if ndim == 3:
+        out += [(((z + 1) % lz) * ly + y) * lh + j, (((z - 1) % lz) * ly + y) * lh + j]
+    return out
+
+
+def components_min(n, edges):
+    parent = list(range(n))
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for a, b in edges:
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
+    return np.array([find(x) for x in range(n)])
+
+
+@pytest.mark.parametrize("shape,beta", [((16, 32), 0.3), ((16, 32), 0.7), ((24, 40), 0.44),
+                                        ((8, 8, 16), 0.22), ((8, 8, 16), 0.5)])
+def test_labels_are_the_components_of_the_active_bonds(oracle_mod, shape, beta):
+    from pyising_b200.backend import B200Int8
+
+    sim = B200Int8(shape, beta, seed=77, init=oracle_mod.random_lattice(shape, 5))
+    sim.sweep(3)
+    c0, c1 = sim.colour_arrays()
+    labels, bonds = sim.cluster_labels(step=9)
+    rows, lh = c0.shape
+    S = rows * lh
+    edges, aligned, active = [], 0, 0
+    for r in range(rows):
+        for j in range(lh):
+            nbs = neighbours(shape, r, j)
+            for k, m in enumerate(nbs):
+                same = c0[r, j] == c1.reshape(-1)[m]
+                aligned += int(same)
+                if bonds[r, j] >> k & 1:
+                    assert same, "an active bond joins anti-aligned spins"
+                    active += 1
+                    edges.append((r * lh + j, S + m))
+            assert bonds[r, j] >> len(nbs) == 0
+    want = components_min(2 * S, edges)
+    np.testing.assert_array_equal(labels.reshape(-1), want)
+    p = 1.0 - math.exp(-2.0 * beta)
+    assert abs(active - p * aligned) < 5 * math.sqrt(aligned * p * (1 - p)) + 1
+
+
+def test_cluster_sweeps_are_deterministic_and_keep_the_lattice_valid():
+    from pyising_b200.backend import B200Int8
+
+    runs = []
+    for _ in range(2):
+        sim = B200Int8((64, 64), 0.44, seed=3, init="cold")
+        sim.cluster_sweep(20)
+        runs.append(sim.get_lattice())
+    np.testing.assert_array_equal(runs[0], runs[1])
+    assert set(np.unique(runs[0])) <= {-1, 1}
+    sim = B200Int8((64, 64), 0.0, seed=3, init="cold")  # beta = 0: no bonds, every spin random
+    sim.cluster_sweep(1)
+    assert abs(sim.get_lattice().mean()) < 0.1
+
+
+@pytest.mark.parametrize("T", [2.0, 2.269185314213022, 3.0])
+def test_cluster_dynamics_sample_the_exact_energy(T):
+    from pyising_b200.backend import B200Int8
+    from pyising_b200.physics import binning_error, energy_torus
+
+    L = 32
+    sim = B200Int8((L, L), 1.0 / T, seed=1234, init="cold")
+    sim.cluster_sweep(200)
+    e = []
+    for _ in range(3000):
+        sim.cluster_sweep(1)
+        e.append(sim.observables_int()[1] / L**2)
+    e = np.array(e)
+    err = binning_error(e)
+    assert abs(e.mean() - energy_torus(T, L)) < 4.5 * err, (e.mean(), energy_torus(T, L), err)
