@@ -158,11 +158,13 @@ int ising_time_sweeps(ising_sim* h, uint64_t t0, int64_t n_sweeps, float* ms);
  * are active when a Philox uniform is below p_bond (the integer threshold of
  * p = 1 - exp(-2 beta)), the connected clusters are found on the device by a lock-free
  * union-find, and each cluster flips with probability 1/2.  Labels take 4 bytes per site,
- * allocated on the first call.  ISING_ERR_TIMEOUT if a bounded union-find loop gave up.
+ * allocated on the first call.  With series_out non-null, the exact (M, E) after every step
+ * lands in series_out[2k], series_out[2k+1] (the call then blocks until done).
+ * ISING_ERR_TIMEOUT if a bounded union-find loop gave up.
  * Replaces: the CPU Wolff sampler used for equilibrated starts and Binder scans
  * (src/pyising/cluster.py:32-104; src/pyising/validate.py:45-50,127-150). */
 int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps, uint64_t seed,
-                        uint32_t p_bond);
+                        uint32_t p_bond, int64_t* series_out);
 
 /* One labeling of step `step` without the flips (diagnostics and tests): labels_out (2*S
  * int32, S = sites per colour; site g = c*S + row*Lx/2 + j) gets each site's cluster root,

@@ -49,7 +49,7 @@ SIGNATURES: dict[str, tuple] = {
     "ising_sweep_static": (I, [I, PI64, I, I, U64, P, I, P, P, U64, I64, I64, P, P]),
     "ising_fill_philox": (I, [P, U64]),
     "ising_set_schedule": (I, [P, I, I]),
-    "ising_cluster_sweep": (I, [P, U64, I64, U64, U32]),
+    "ising_cluster_sweep": (I, [P, U64, I64, U64, U32, P]),
     "ising_cluster_labels": (I, [P, U64, U64, U32, P, P]),
     "ising_set_knob": (I, [P, I, I]),
     "ising_get_knob": (I, [P, I, ctypes.POINTER(I)]),

@@ -211,17 +211,21 @@ class B200Int8(_B200Simulation):
 
         return prob_to_threshold(1.0 - math.exp(-2.0 * self.beta)) if self.beta > 0 else 0
 
-    def cluster_sweep(self, n: int = 1, seed: int | None = None) -> None:
+    def cluster_sweep(self, n: int = 1, seed: int | None = None,
+                      measure: bool = False) -> np.ndarray | None:
         """``n`` Swendsen-Wang updates (steps ``self.cluster_t`` ..), keyed by ``seed`` (the
         simulation's seed by default).  The Metropolis/heat-bath sweep counter ``t`` is not
-        touched; the cluster step counter ``cluster_t`` advances by ``n``."""
+        touched; the cluster step counter ``cluster_t`` advances by ``n``.  With ``measure``,
+        returns the exact ``(M, E)`` after every step as an ``(n, 2)`` int64 array."""
         n = int(n)
         if n <= 0:
-            return
+            return np.zeros((0, 2), np.int64) if measure else None
         key = self.seed if seed is None else int(seed) & 0xFFFFFFFFFFFFFFFF
-        check(lib().ising_cluster_sweep(self._h, self.cluster_t, n, key, self.bond_threshold()),
-              "cluster_sweep")
+        out = np.zeros((n, 2), np.int64) if measure else None
+        check(lib().ising_cluster_sweep(self._h, self.cluster_t, n, key, self.bond_threshold(),
+                                        out.ctypes.data if measure else None), "cluster_sweep")
         self.cluster_t += n
+        return out
 
     def cluster_labels(self, step: int = 0, seed: int | None = None) -> tuple[np.ndarray,
                                                                               np.ndarray]:

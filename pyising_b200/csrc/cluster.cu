@@ -209,7 +209,7 @@ static int cluster_error(ising_sim* h)
 using namespace ising;
 
 extern "C" int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps, uint64_t seed,
-                                   uint32_t p_bond)
+                                   uint32_t p_bond, int64_t* series_out)
 {
     if (!h) return fail(ISING_ERR_INVALID, "null handle");
     if (n_steps < 0) return fail(ISING_ERR_INVALID, "negative step count");
@@ -217,15 +217,30 @@ extern "C" int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     int rc = cluster_setup(h);
     if (rc != ISING_OK) return rc;
+    if (series_out && n_steps > 0) {
+        rc = ensure_series(h, n_steps);
+        if (rc != ISING_OK) return rc;
+        e = cudaMemsetAsync(h->d_series, 0, (size_t)n_steps * 2 * sizeof(long long), h->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync (series)");
+    }
     const long long S = h->rows * (long long)h->lh;
     e = cudaMemsetAsync(reinterpret_cast<char*>(h->d_label) + 2 * S * sizeof(int), 0, sizeof(int),
                         h->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     for (int64_t k = 0; k < n_steps; ++k) {
         rc = cluster_step(h, (u32)(step0 + (uint64_t)k), seed, p_bond, true, nullptr);
+        if (rc == ISING_OK && series_out)
+            rc = observe(h, reinterpret_cast<unsigned long long*>(h->d_series + 2 * k));
         if (rc != ISING_OK) return rc;
     }
-    return cluster_error(h);
+    rc = cluster_error(h);
+    if (rc == ISING_OK && series_out && n_steps > 0) {
+        e = cudaMemcpyAsync(series_out, h->d_series, (size_t)n_steps * 2 * sizeof(long long),
+                            cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cluster series copy");
+    }
+    return rc;
 }
 
 extern "C" int ising_cluster_labels(ising_sim* h, uint64_t step, uint64_t seed, uint32_t p_bond,

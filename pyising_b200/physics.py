@@ -169,15 +169,49 @@ class Summary:
                    binder(m), jackknife_binder_error(m), int(len(s)))
 
 
+# ------------------------------------------------------------------ cluster updates ------
+def equilibrated(shape, T: float, seed: int, steps: int = 300) -> np.ndarray:
+    """An equilibrium start: ``steps`` Swendsen-Wang updates on the device from a cold start
+    (pyising equilibrates with CPU Wolff updates, src/pyising/validate.py:45-50)."""
+    from .backend import B200Int8
+
+    sim = B200Int8(tuple(shape), 1.0 / T, seed=seed, init="cold")
+    sim.cluster_sweep(steps)
+    return sim.get_lattice()
+
+
+def cluster_binder_scan(Ls, Ts, therm: int, meas: int, dim: int = 2, seed: int = 21) -> dict:
+    """Binder cumulants from Swendsen-Wang chains (one lattice per (L, T), (M, E) after every
+    update measured on the device) and the crossings of consecutive sizes; the cluster dynamics
+    decorrelate near T_c in a few updates, as pyising's Wolff scans do
+    (src/pyising/validate.py:127-150)."""
+    from .backend import B200Int8
+
+    Ts = [float(t) for t in Ts]
+    u = {L: [0.0] * len(Ts) for L in Ls}
+    err = {L: [0.0] * len(Ts) for L in Ls}
+    for a, L in enumerate(Ls):
+        for i, T in enumerate(Ts):
+            sim = B200Int8((L,) * dim, 1.0 / T, seed=seed + 1000 * a + i, init="cold")
+            sim.cluster_sweep(therm)
+            s = Summary.from_series(sim.cluster_sweep(meas, measure=True), L ** dim)
+            u[L][i], err[L][i] = s.binder, s.binder_err
+    crossings = {f"{a}-{b}": crossing(Ts, u[a], u[b]) for a, b in zip(Ls, Ls[1:])}
+    return {"T": Ts, "U4": u, "U4_err": err, "crossings": crossings}
+
+
 # ------------------------------------------------------------------ batched scans --------
 def temperature_scan(L: int, Ts, therm: int, meas: int, every: int,
                      kinds=(("int8", "metropolis"), ("msc", "metropolis"),
-                            ("int8", "heatbath")), seed: int = 7, dim: int = 2) -> list[dict]:
+                            ("int8", "heatbath")), seed: int = 7, dim: int = 2,
+                     equilibrate: int = 0) -> list[dict]:
     """Every (kind, T) of a scan as one batched ensemble; returns a row per lattice with the
     estimates and, in 2D, the exact finite-torus energy and the Onsager-Yang magnetisation.
 
     Each lattice gets its own seed (seed + 1000 k + i): with one shared seed the counter-based
-    uniforms would be identical at every temperature and the errors would correlate."""
+    uniforms would be identical at every temperature and the errors would correlate.  With
+    ``equilibrate`` > 0 every lattice starts from that many Swendsen-Wang updates
+    (:func:`equilibrated`), else ordered below T_c and disordered above."""
     from .ensemble import Ensemble, Job
 
     shape = (L,) * dim
@@ -185,11 +219,14 @@ def temperature_scan(L: int, Ts, therm: int, meas: int, every: int,
     jobs, keys = [], []
     for k, (variant, alg) in enumerate(kinds):
         for i, T in enumerate(Ts):
-            # ordered start below T_c (a hot start can freeze into a long-lived striped state
-            # there), device seeded disordered start above
+            if equilibrate > 0:
+                init = equilibrated(shape, T, seed=int(1000 * T) + k, steps=equilibrate)
+            else:
+                # ordered start below T_c (a hot start can freeze into a long-lived striped
+                # state there), device seeded disordered start above
+                init = "cold" if T < tc else "philox"
             jobs.append(Job(shape, 1.0 / T, therm + meas * every, seed=seed + 1000 * k + i,
-                            variant=variant, algorithm=alg, measure_every=every,
-                            init="cold" if T < tc else "philox"))
+                            variant=variant, algorithm=alg, measure_every=every, init=init))
             keys.append((variant, alg, float(T)))
     rows = []
     with Ensemble() as ens:

@@ -10,10 +10,13 @@ temperature, kind), each bit-identical to running it alone:
 2. 2D Binder-cumulant crossings of several sizes vs Onsager's T_c.
 3. 3D Binder-cumulant crossings vs the simple-cubic critical coupling (Ferrenberg, Xu & Landau).
 4. 3D Metropolis vs heat bath energies (two different Markov chains, one equilibrium).
+5. 2D and 3D Binder crossings again from Swendsen-Wang cluster chains on the device.
 
-The reference runs the Binder scans and the 3D comparison with a CPU Wolff sampler
-(src/pyising/validate.py:127-178); here every chain is a local-update chain on the GPU, long
-enough near T_c to outlast its autocorrelation.  Bitwise identity against the NumPy oracle is
+The reference equilibrates its starts and runs its Binder scans and 3D comparison with a CPU
+Wolff sampler (src/pyising/validate.py:45-50,127-178); here the starts come from Swendsen-Wang
+updates on the device (item 1), the batched local-update chains run long enough near T_c to
+outlast their autocorrelation (items 2-4), and item 5 repeats the crossings with cluster
+chains.  Bitwise identity against the NumPy oracle is
 the job of the test suite (tests/), which is where the oracle may be imported.
 """
 
@@ -39,6 +42,8 @@ QUICK = {
     "binder3_L": [8, 16], "binder3_T": list(np.linspace(4.45, 4.57, 5)),
     "binder3_therm": 4000, "binder3_meas": 20000, "binder3_every": 2,
     "L3": 16, "T3": [4.0, TC_3D, 5.0],
+    "equilibrate": 100, "cluster2_L": [8, 16], "cluster3_L": [8, 16], "cluster_therm": 100,
+    "cluster_meas": 2000,
 }
 FULL = {
     "L2": 128, "T2": sorted(list(np.round(np.linspace(1.6, 3.4, 19), 3)) + [TC_2D]),
@@ -48,6 +53,8 @@ FULL = {
     "binder3_L": [8, 16, 32], "binder3_T": list(np.round(np.linspace(4.47, 4.55, 9), 4)),
     "binder3_therm": 20000, "binder3_meas": 50000, "binder3_every": 5,
     "L3": 32, "T3": [3.5, 4.2, TC_3D, 5.0, 6.0],
+    "equilibrate": 300, "cluster2_L": [8, 16, 32, 64], "cluster3_L": [8, 16, 32],
+    "cluster_therm": 200, "cluster_meas": 10000,
 }
 
 
@@ -63,7 +70,7 @@ def scan_2d(cfg: dict, log=print) -> list[dict]:
     for Ts, mult in ((far, 1), (near, 4)):
         if Ts:
             rows += temperature_scan(cfg["L2"], Ts, cfg["therm"], cfg["meas"] * mult,
-                                     cfg["every"])
+                                     cfg["every"], equilibrate=cfg["equilibrate"])
     rows.sort(key=lambda r: (r["variant"], r["algorithm"], r["T"]))
     for r in rows:
         log(f"  2D {r['variant']:<5} {r['algorithm']:<10} T={r['T']:.4f} |m|={r['abs_m']:.5f} "
@@ -88,6 +95,25 @@ def binder(cfg: dict, dim: int, log=print) -> dict:
     out["U4_err"] = {str(L): v for L, v in out["U4_err"].items()}
     for pair, tc in out["crossings"].items():
         log(f"  Binder crossing {dim}D L={pair}: T = {tc:.5f} (reference {ref:.5f})")
+    return out
+
+
+def cluster_binder(cfg: dict, dim: int, log=print) -> dict:
+    """Items 2 and 3 again with Swendsen-Wang chains on the device, at the reference's sizes
+    (its Wolff scans, src/pyising/validate.py:127-150)."""
+    from .physics import cluster_binder_scan
+
+    Ls = cfg[f"cluster{dim}_L"]
+    out = cluster_binder_scan(Ls, cfg[f"binder{dim}_T"], cfg["cluster_therm"],
+                              cfg["cluster_meas"], dim=dim)
+    ref = TC_2D if dim == 2 else TC_3D
+    est = out["crossings"][f"{Ls[-2]}-{Ls[-1]}"]
+    out.update({"dim": dim, "L": Ls, "Tc_reference": ref, "Tc_estimate": est,
+                "Tc_rel_error": abs(est - ref) / ref, "updates": "Swendsen-Wang"})
+    out["U4"] = {str(L): v for L, v in out["U4"].items()}
+    out["U4_err"] = {str(L): v for L, v in out["U4_err"].items()}
+    for pair, tc in out["crossings"].items():
+        log(f"  Swendsen-Wang Binder crossing {dim}D L={pair}: T = {tc:.5f} (reference {ref:.5f})")
     return out
 
 
@@ -128,6 +154,10 @@ def summarize(res: dict) -> dict:
         "Tc3d_estimate": res["binder3d"]["Tc_estimate"],
         "Tc3d_rel_error": res["binder3d"]["Tc_rel_error"],
         "e3d_max_abs_z_metropolis_vs_heatbath": max(abs(r["e_z"]) for r in res["scan3d"]),
+        "Tc2d_cluster_estimate": res["binder2d_cluster"]["Tc_estimate"],
+        "Tc2d_cluster_rel_error": res["binder2d_cluster"]["Tc_rel_error"],
+        "Tc3d_cluster_estimate": res["binder3d_cluster"]["Tc_estimate"],
+        "Tc3d_cluster_rel_error": res["binder3d_cluster"]["Tc_rel_error"],
     }
 
 
@@ -136,14 +166,17 @@ def run(quick: bool = False, out: str | Path | None = None, log=print) -> dict:
     cfg = QUICK if quick else FULL
     t0 = time.time()
     res: dict = {"quick": quick, "config": cfg, "beta_c_3d": BETA_C_3D}
-    log("[1/4] 2D energy and magnetisation vs exact results")
+    log("[1/5] 2D energy and magnetisation vs exact results (Swendsen-Wang equilibrated starts)")
     res["scan2d"] = scan_2d(cfg, log)
-    log("[2/4] 2D Binder crossing")
+    log("[2/5] 2D Binder crossing")
     res["binder2d"] = binder(cfg, 2, log)
-    log("[3/4] 3D Binder crossing")
+    log("[3/5] 3D Binder crossing")
     res["binder3d"] = binder(cfg, 3, log)
-    log("[4/4] 3D Metropolis vs heat bath")
+    log("[4/5] 3D Metropolis vs heat bath")
     res["scan3d"] = scan_3d(cfg, log)
+    log("[5/5] 2D and 3D Binder crossings from Swendsen-Wang chains")
+    res["binder2d_cluster"] = cluster_binder(cfg, 2, log)
+    res["binder3d_cluster"] = cluster_binder(cfg, 3, log)
     res["summary"] = summarize(res)
     res["seconds"] = time.time() - t0
     log(json.dumps(res["summary"]))

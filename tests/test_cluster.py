@@ -109,3 +109,17 @@ def test_cluster_dynamics_sample_the_exact_energy(T):
     e = np.array(e)
     err = binning_error(e)
     assert abs(e.mean() - energy_torus(T, L)) < 4.5 * err, (e.mean(), energy_torus(T, L), err)
+
+
+def test_measured_cluster_series_and_binder_scan():
+    from pyising_b200.backend import B200Int8
+    from pyising_b200.physics import TC_2D, cluster_binder_scan, equilibrated
+
+    sim = B200Int8((32, 32), 0.44, seed=8, init="cold")
+    series = sim.cluster_sweep(50, measure=True)
+    assert series.shape == (50, 2) and sim.cluster_t == 50
+    assert tuple(series[-1]) == sim.observables_int()
+    lat = equilibrated((32, 32), 2.0, seed=4, steps=50)
+    assert abs(abs(lat.mean()) - 0.9113) < 0.06  # ordered at T = 2.0
+    out = cluster_binder_scan([8, 16], [2.15, 2.25, 2.35, 2.45], therm=100, meas=3000)
+    assert abs(out["crossings"]["8-16"] - TC_2D) < 0.08, out
