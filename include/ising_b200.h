@@ -114,7 +114,10 @@ int ising_half_sweep(ising_sim* h, int color, uint64_t t);
  *   ISING_SCHEDULE_LAUNCHES   one kernel launch per half-sweep;
  *   ISING_SCHEDULE_GRAPHS     replayed CUDA graphs of whole chunks of sweeps;
  *   ISING_SCHEDULE_PERSISTENT one cooperative launch for all sweeps (2D int8; others fall back):
- *                             bands of rows wait only for their neighbours, every wait bounded.
+ *                             bands of rows wait only for their neighbours, every wait bounded;
+ *   ISING_SCHEDULE_TEMPORAL   graphs whose launches each run two unmeasured sweeps on
+ *                             shared-memory tiles with recomputed halos (small 2D int8
+ *                             lattices with rows a multiple of 16 bytes; others fall back).
  * All schedules give identical results.  test_mute_band >= 0 makes that band of a persistent
  * run stop publishing its progress, so its neighbours' bounded waits expire: the sweep then
  * reports ISING_ERR_TIMEOUT (the lattice is no longer valid); pass -1 otherwise. */
@@ -122,6 +125,7 @@ int ising_half_sweep(ising_sim* h, int color, uint64_t t);
 #define ISING_SCHEDULE_LAUNCHES 1
 #define ISING_SCHEDULE_GRAPHS 2
 #define ISING_SCHEDULE_PERSISTENT 3
+#define ISING_SCHEDULE_TEMPORAL 4
 int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
 
 /* Launch knobs of a handle, picked by the autotuner (pyising_b200.autotune) or by hand.  Every

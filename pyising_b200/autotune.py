@@ -9,7 +9,8 @@ by site, sweep and colour, and every schedule visits the same sites with the sam
 * ``blocks_per_sm`` grid size in blocks of 256 threads per SM;
 * ``msc_waves``     msc: contiguous warp ranges per resident warp of the work-stack kernel;
 * ``graph_chunk``   sweeps per captured CUDA graph of an unmeasured run;
-* ``schedule``      ``"auto"`` (graphs), ``"launches"`` or ``"persistent"`` (2D int8).
+* ``schedule``      ``"auto"`` (graphs), ``"launches"``, ``"persistent"`` or ``"temporal"``
+                    (2D int8: two sweeps per launch on shared-memory tiles).
 
 :func:`tune` measures them on a scratch lattice of the given shape (device seeded start, CUDA
 events on the simulation's stream) by coordinate descent from the defaults, and stores the best
@@ -78,6 +79,8 @@ def search_space(variant: str, shape, algorithm: str = "metropolis") -> dict[str
     space["blocks_per_sm"] = [8, 4, 16]
     if variant == "int8" and len(shape) == 2:
         space["schedule"] = ["auto", "launches", "persistent"]
+        if lh % 16 == 0 and shape[0] % 8 == 0 and shape[0] >= 16 and 32 * lh <= 96 * 1024:
+            space["schedule"].append("temporal")
     else:
         space["schedule"] = ["auto", "launches"]
     space["graph_chunk"] = [32, 8, 128]

@@ -129,12 +129,13 @@ class _B200Simulation(IsingSimulation):
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         check(lib().ising_set_seed(self._h, self.seed), "set_seed")
 
-    SCHEDULES = {"auto": 0, "launches": 1, "graphs": 2, "persistent": 3}
+    SCHEDULES = {"auto": 0, "launches": 1, "graphs": 2, "persistent": 3, "temporal": 4}
 
     def set_schedule(self, schedule: str = "auto", test_mute_band: int = -1) -> None:
         """How sweeps are issued: ``"auto"``, ``"launches"`` (one kernel per half-sweep),
-        ``"graphs"`` (replayed CUDA graphs) or ``"persistent"`` (one cooperative launch for all
-        sweeps; 2D int8).  Results are identical.  ``test_mute_band`` >= 0 is a test hook that
+        ``"graphs"`` (replayed CUDA graphs), ``"persistent"`` (one cooperative launch for all
+        sweeps; 2D int8) or ``"temporal"`` (graphs of launches that each run two sweeps on
+        shared-memory tiles; small 2D int8 lattices).  Results are identical.  ``test_mute_band`` >= 0 is a test hook that
         makes one band of a persistent run stop publishing, so the run reports a time-out."""
         check(lib().ising_set_schedule(self._h, self.SCHEDULES[schedule], int(test_mute_band)),
               "set_schedule")

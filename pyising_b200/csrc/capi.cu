@@ -110,11 +110,19 @@ static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* 
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
     int rc = ISING_OK;
-    for (int64_t s = 0; s < G && rc == ISING_OK; ++s) {
+    const bool tb = h->schedule == ISING_SCHEDULE_TEMPORAL && temporal_ok(h);
+    for (int64_t s = 0; s < G && rc == ISING_OK;) {
+        if (tb && s + 2 <= G - (measured ? 1 : 0)) {  // two unmeasured sweeps in one launch
+            const cudaError_t le = launch_int8_temporal(h, (u32)s, ctl);
+            if (le != cudaSuccess) rc = cuda_fail(le, "temporal half-sweeps");
+            s += 2;
+            continue;
+        }
         unsigned long long* m =
             (measured && s == G - 1) ? (unsigned long long*)h->d_series : nullptr;
         rc = half_sweep(h, 0, (u32)s, nullptr, nullptr, ctl);
         if (rc == ISING_OK) rc = half_sweep(h, 1, (u32)s, m, nullptr, ctl);
+        ++s;
     }
     if (rc == ISING_OK) {
         ctl_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_acc + 6, (unsigned long long)G,
@@ -467,7 +475,7 @@ int ising_fill_philox(ising_sim* h, uint64_t start_seed)
 int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band)
 {
     CHECK_HANDLE(h);
-    if (schedule < ISING_SCHEDULE_AUTO || schedule > ISING_SCHEDULE_PERSISTENT)
+    if (schedule < ISING_SCHEDULE_AUTO || schedule > ISING_SCHEDULE_TEMPORAL)
         return fail(ISING_ERR_INVALID, "unknown schedule %d", schedule);
     h->schedule = schedule;
     h->mute_band = test_mute_band;
@@ -634,9 +642,16 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
             s0 = n_sweeps;
         }
     }
+    const bool tb = h->schedule == ISING_SCHEDULE_TEMPORAL && temporal_ok(h);
     for (int64_t s = s0; s < n_sweeps; ++s) {
         const u32 t = (u32)(t0 + (uint64_t)s);
         const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;
+        if (tb && !meas && s + 2 <= n_sweeps &&
+            !(measure_every > 0 && (s + 2) % measure_every == 0)) {
+            TRY_CUDA(launch_int8_temporal(h, t, nullptr));  // sweeps s and s + 1
+            ++s;
+            continue;
+        }
         unsigned long long* m = meas ? (unsigned long long*)(h->d_series + 2 * k) : nullptr;
         int rc = half_sweep(h, 0, t, nullptr, nullptr);
         if (rc == ISING_OK) rc = half_sweep(h, 1, t, m, nullptr);

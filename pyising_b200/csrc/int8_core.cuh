@@ -167,13 +167,18 @@ __device__ __forceinline__ u32 decide4(const Int8Half& p, u32 s, u32 cnt, const 
 // instructions as a full one (no divergence inside a warp), with the padding words selected
 // away: their random numbers are drawn and discarded, their bytes stored back unchanged, and
 // the right-hand neighbour of the last valid word is the row's wrapped edge byte.
-template <int V, int NDIM, int RULE, bool MIXED, bool MEAS>
-__device__ __forceinline__ void int8_update(const Int8Half& p, long long row, int par, int j0,
-                                            int wv, const Words<V / 4>& s, const Words<V / 4>& c,
-                                            const Words<V / 4>& nu, const Words<V / 4>& nd,
-                                            const Words<V / 4>& zu, const Words<V / 4>& zd,
-                                            u32 edge, const u32* stab, long long& m_acc,
-                                            long long& e_acc)
+// Returns the new words; STORE = false leaves storing them to the caller (the tiles of the
+// temporally blocked kernel live in shared memory).
+template <int V, int NDIM, int RULE, bool MIXED, bool MEAS, bool STORE = true>
+__device__ __forceinline__ Words<V / 4> int8_update(const Int8Half& p, long long row, int par,
+                                                    int j0, int wv, const Words<V / 4>& s,
+                                                    const Words<V / 4>& c,
+                                                    const Words<V / 4>& nu,
+                                                    const Words<V / 4>& nd,
+                                                    const Words<V / 4>& zu,
+                                                    const Words<V / 4>& zd, u32 edge,
+                                                    const u32* stab, long long& m_acc,
+                                                    long long& e_acc)
 {
     constexpr int W = V / 4;
     constexpr bool kHeat = (RULE == kHeatFast || RULE == kHeatGeneric);
@@ -227,7 +232,7 @@ __device__ __forceinline__ void int8_update(const Int8Half& p, long long row, in
             ns.v[k] = (!MIXED || k < wv) ? d : s.v[k];
         }
     }
-    if constexpr (RULE != kObserve) store_words<W>(p.own + row * p.pitch + j0, ns);
+    if constexpr (RULE != kObserve && STORE) store_words<W>(p.own + row * p.pitch + j0, ns);
 
     if constexpr (MEAS) {
         // Bonds of this colour's sites: s*h = 2d - 2A' per site (A' = anti-aligned neighbours
@@ -251,6 +256,7 @@ __device__ __forceinline__ void int8_update(const Int8Half& p, long long row, in
         m_acc += 2 * nv - 2 * (down + other_down);  // this colour's sites + the other's
         e_acc += 2 * anti - 2 * NDIM * nv;          // -(2d n - 2 anti)
     }
+    return ns;
 }
 
 template <bool MIXED, int W>

@@ -23,6 +23,8 @@ BETA_C_2D = 0.44068679350977147
     ((6, 32), "heatbath", 0.42),        # fewer rows than SMs
     ((512, 1024), "heatbath", 0.44),
     ((48, 96), "heatbath", -0.3),       # non-monotone table: lookup rule
+    ((32, 64), "heatbath", 0.42),       # temporal tiles: Ly = 2 bands + halo
+    ((16, 2048), "metropolis", 0.44),   # temporal tiles: Ly = the smallest allowed
 ])
 def test_schedules_match_oracle(oracle_mod, shape, algorithm, beta):
     from pyising_b200.backend import B200Int8
@@ -31,12 +33,28 @@ def test_schedules_match_oracle(oracle_mod, shape, algorithm, beta):
     ref = oracle_mod.OracleInt8(shape, beta, seed=2**40 + 9, algorithm=algorithm, init=lat)
     want = ref.sweep(40, measure_every=5)
     ref.sweep(11)
-    for schedule in ("launches", "graphs", "persistent", "auto"):
+    for schedule in ("launches", "graphs", "persistent", "temporal", "auto"):
         sim = B200Int8(shape, beta, seed=2**40 + 9, algorithm=algorithm, init=lat)
         sim.set_schedule(schedule)
         np.testing.assert_array_equal(sim.sweep_measured(40, 5), want, err_msg=schedule)
         sim.sweep(11)
         np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice(), err_msg=schedule)
+
+
+def test_temporal_c1_golden():
+    """C1 on the temporally blocked schedule (two sweeps per launch between measurements)."""
+    from pyising_b200.backend import B200Int8
+
+    g = golden("c1_int8_L1024.npz")
+    sim = B200Int8((1024, 1024), float(g["beta"]), seed=1, init="hot")
+    sim.set_schedule("temporal")
+    np.testing.assert_array_equal(sim.sweep_measured(1000, 100), g["series"])
+    np.testing.assert_array_equal(sim.get_lattice(), unpack_lattice(g["final"], (1024, 1024)))
+    sim2 = B200Int8((1024, 1024), float(g["beta"]), seed=1, init="hot")
+    sim2.set_schedule("temporal")
+    sim2.sweep(999)  # odd count: a graph chunk tail and one single sweep
+    sim2.sweep(1)
+    np.testing.assert_array_equal(sim2.get_lattice(), unpack_lattice(g["final"], (1024, 1024)))
 
 
 def test_persistent_c1_golden():
