@@ -110,7 +110,8 @@ int ising_half_sweep(ising_sim* h, int color, uint64_t t);
 
 /* How ising_sweep issues its half-sweeps (no counterpart in the reference, which launches one
  * kernel per half-sweep from Python):
- *   ISING_SCHEDULE_AUTO       graphs for whole chunks of sweeps, launches for the rest;
+ *   ISING_SCHEDULE_AUTO       graphs for whole chunks of sweeps, launches for the rest (the
+ *                             temporal tiles below for eligible lattices up to 1024^2);
  *   ISING_SCHEDULE_LAUNCHES   one kernel launch per half-sweep;
  *   ISING_SCHEDULE_GRAPHS     replayed CUDA graphs of whole chunks of sweeps;
  *   ISING_SCHEDULE_PERSISTENT one cooperative launch for all sweeps (2D int8; others fall back):

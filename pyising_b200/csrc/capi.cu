@@ -97,6 +97,18 @@ void clear_graphs(ising_sim* h)
     h->graphs.clear();
 }
 
+// Two unmeasured sweeps per launch on shared-memory tiles: when asked for, and by default for
+// eligible lattices of up to 512K sites per colour (1024^2), where a half-sweep is too short to
+// hide its launch (larger ones measured faster with single half-sweeps).
+constexpr long long kTemporalAutoSites = 512 * 1024;
+
+static bool use_temporal(const ising_sim* h)
+{
+    if (!temporal_ok(h)) return false;
+    if (h->schedule == ISING_SCHEDULE_TEMPORAL) return true;
+    return h->schedule == ISING_SCHEDULE_AUTO && h->rows * (long long)h->lh <= kTemporalAutoSites;
+}
+
 // The captured chunk of G sweeps of this handle: 2G half-sweeps with counters relative to the
 // control block d_acc[6] (sweep) / d_acc[7] (series slot), then one node advancing it.
 static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* out)
@@ -110,7 +122,7 @@ static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* 
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
     int rc = ISING_OK;
-    const bool tb = h->schedule == ISING_SCHEDULE_TEMPORAL && temporal_ok(h);
+    const bool tb = use_temporal(h);
     for (int64_t s = 0; s < G && rc == ISING_OK;) {
         if (tb && s + 2 <= G - (measured ? 1 : 0)) {  // two unmeasured sweeps in one launch
             const cudaError_t le = launch_int8_temporal(h, (u32)s, ctl);
@@ -642,7 +654,7 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
             s0 = n_sweeps;
         }
     }
-    const bool tb = h->schedule == ISING_SCHEDULE_TEMPORAL && temporal_ok(h);
+    const bool tb = use_temporal(h);
     for (int64_t s = s0; s < n_sweeps; ++s) {
         const u32 t = (u32)(t0 + (uint64_t)s);
         const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;

@@ -14,7 +14,7 @@
 //      u32 from Philox((n, t, kBondTag, k), key)); active bonds union their endpoints' trees:
 //      roots are linked larger-under-smaller with atomicCAS, finds halve paths with plain
 //      stores (parents only ever move up the tree, so a stale read is still an ancestor);
-//   3. every label is replaced by its root;
+//   3. every label is replaced by its root (a read-only walk: only thread i writes label[i]);
 //   4. every cluster flips with probability 1/2: bit (root & 127) of
 //      Philox((root >> 7, t, kFlipTag, 0), key), the same for all its sites.
 // Site g = c * S + row * lh + j (S = rows * lh sites per colour, the logical compressed index).
@@ -48,6 +48,19 @@ __device__ __forceinline__ int uf_find(int* label, int x, int* err)
         const int gp = __ldcg(label + p);
         if (gp != p) label[x] = gp;  // path halving
         x = gp;
+    }
+    atomicExch(err, 1);
+    return x;
+}
+
+// The root of x without writing anything: flattening must not halve paths, or a halving store
+// (label[x] = grandparent) could overwrite the root another thread has just written to label[x].
+__device__ __forceinline__ int uf_root(const int* label, int x, int* err)
+{
+    for (long long it = 0; it < kFindLimit; ++it) {
+        const int p = __ldcg(label + x);
+        if (p == x) return x;
+        x = p;
     }
     atomicExch(err, 1);
     return x;
@@ -119,11 +132,13 @@ __global__ void sw_bond_kernel(const ClusterArgs a)
     }
 }
 
+// Every label becomes its root; only thread i writes label[i], and every value it can hold
+// meanwhile (its old parent or the root) is an ancestor, so other threads' walks stay valid.
 __global__ void sw_flatten_kernel(int* label, long long n, int* err)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
-        label[i] = uf_find(label, (int)i, err);
+        label[i] = uf_root(label, (int)i, err);
 }
 
 __global__ void sw_flip_kernel(const ClusterArgs a)

@@ -83,11 +83,12 @@ def test_cluster_sweeps_are_deterministic_and_keep_the_lattice_valid():
     from pyising_b200.backend import B200Int8
 
     runs = []
-    for _ in range(2):
-        sim = B200Int8((64, 64), 0.44, seed=3, init="cold")
-        sim.cluster_sweep(20)
+    for _ in range(3):  # the union order varies between runs; the clusters must not
+        sim = B200Int8((256, 256), 0.44, seed=3, init="cold")
+        sim.cluster_sweep(40)
         runs.append(sim.get_lattice())
     np.testing.assert_array_equal(runs[0], runs[1])
+    np.testing.assert_array_equal(runs[0], runs[2])
     assert set(np.unique(runs[0])) <= {-1, 1}
     sim = B200Int8((64, 64), 0.0, seed=3, init="cold")  # beta = 0: no bonds, every spin random
     sim.cluster_sweep(1)
