@@ -1,9 +1,10 @@
 """Run one small sweep case, for profilers (ncu) and quick timing.
 
-    python -m pyising_b200.profile_case {int8|hb3|msc|batch} L SWEEPS
+    python -m pyising_b200.profile_case {int8|hb3|msc|sw|batch} L SWEEPS
 
 int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
 beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7;
+sw: SWEEPS Swendsen-Wang updates of a 2D int8 L x L lattice at beta_c from a cold start;
 batch: an ensemble of 2D int8 Metropolis lattices L x L, L/2 x L/2 (four each) and L/4 x L/4
 (sixteen) at temperatures 2.0 .. 2.6, device seeded starts, SWEEPS sweeps with (M, E) every 10,
 through the batched kernel.  Prints the final exact (M, E) (batch: of the first lattice).
@@ -25,6 +26,12 @@ def main(argv: list[str]) -> int:
         sim = B200Int8((L, L, L), 0.221654626, seed=0, algorithm="heatbath", init="cold")
     elif which == "msc":
         sim = B200MultiSpin((L, L), BETA_C_2D, seed=7, init="hot")
+    elif which == "sw":
+        sim = B200Int8((L, L), BETA_C_2D, seed=7, init="cold")
+        sim.cluster_sweep(n)
+        sim.synchronize()
+        print(which, L, n, sim.observables_int())
+        return 0
     elif which == "batch":
         from .ensemble import Ensemble, Job
 
