@@ -294,6 +294,50 @@ int ising_server_status(ising_server* s, int64_t* pending, int64_t* active, int6
 int ising_server_set_knob(ising_server* s, int knob, int value);
 int ising_server_destroy(ising_server* s);
 
+/* ---- slab decomposition of one lattice over several devices ---------------------------- */
+/* No counterpart in the reference (one lattice lives on one device there).  A slab handle owns
+ * rows [begin, begin + count) of the first axis of the whole lattice `shape` (rows y in 2D,
+ * planes z in 3D) plus one halo row (2D) or plane (3D) of each colour on each side.  A
+ * half-sweep of colour c reads the opposite colour's halos, so before it the caller copies the
+ * opposite colour's edge rows of the neighbouring slabs into them (periodic along the axis), by
+ * NCCL, a peer copy or a local copy; the half-sweep itself never wraps along the slab axis.
+ * Random numbers use global site indices, so the slabs together give exactly the results of one
+ * ising_sim holding the whole lattice, and the lattice's (M, E) is the sum over the slabs.
+ * Per-slab calls mirror ising_create / ising_set_table / ising_upload / ising_download /
+ * ising_fill_cold / ising_fill_philox / ising_half_sweep / ising_observables / ising_sync; host
+ * colour arrays hold the owned rows only ((rows, Lx/2) int8 or (rows, Lx/128) uint64). */
+typedef struct ising_slab ising_slab;
+
+#define ISING_SLAB_HALO_LOW 0   /* halo before owned row 0 (receives the previous slab's edge) */
+#define ISING_SLAB_HALO_HIGH 1  /* halo after the last owned row (the next slab's edge) */
+#define ISING_SLAB_EDGE_LOW 2   /* first owned row or plane (sent to the previous slab) */
+#define ISING_SLAB_EDGE_HIGH 3  /* last owned row or plane (sent to the next slab) */
+
+int ising_slab_create(int ndim, const int64_t* shape, int variant, int algorithm, uint64_t seed,
+                      int64_t begin, int64_t count, int device, ising_slab** out);
+int ising_slab_destroy(ising_slab* s);
+int ising_slab_set_stream(ising_slab* s, void* stream);
+int ising_slab_set_table(ising_slab* s, const uint32_t* table, int n);
+int ising_slab_upload(ising_slab* s, const void* c0, const void* c1);
+int ising_slab_download(ising_slab* s, void* c0, void* c1);
+int ising_slab_fill_cold(ising_slab* s);
+int ising_slab_fill_philox(ising_slab* s, uint64_t start_seed);
+/* Device address and byte count of one halo or edge region of colour `color` (`which`: one of
+ * ISING_SLAB_HALO_* / ISING_SLAB_EDGE_*); the region is contiguous and the same size on every
+ * slab of a lattice. */
+int ising_slab_halo(ising_slab* s, int color, int which, void** ptr, int64_t* bytes);
+/* Zero `pairs` (M, E) slots on the device (allocating them on first use). */
+int ising_slab_series_reset(ising_slab* s, int64_t pairs);
+/* One half-sweep of colour `color` at sweep counter t on the slab's stream; with slot >= 0 the
+ * half-sweep also adds the slab's exact (M, E) after it to series slot `slot` (measure on
+ * colour 1, the second half of a sweep, as ising_sweep does). */
+int ising_slab_half_sweep(ising_slab* s, int color, uint64_t t, int64_t slot);
+/* Copy `pairs` series slots to the host (blocks). */
+int ising_slab_series_read(ising_slab* s, int64_t pairs, int64_t* out);
+/* The slab's (M, E) over its owned sites (blocks); the colour-0 halos must be current. */
+int ising_slab_observables(ising_slab* s, int64_t* m, int64_t* e);
+int ising_slab_sync(ising_slab* s);
+
 /* ---- device probes (roofline ceilings and generator checks) ---------------------------- */
 
 /* Self-test of the bounded device-side wait used by the persistent schedule: one CTA waits for

@@ -72,6 +72,20 @@ SIGNATURES: dict[str, tuple] = {
     "ising_server_release": (I, [P, I64]),
     "ising_server_status": (I, [P, PI64, PI64, PI64, PI64]),
     "ising_server_destroy": (I, [P]),
+    "ising_slab_create": (I, [I, PI64, I, I, U64, I64, I64, I, ctypes.POINTER(P)]),
+    "ising_slab_destroy": (I, [P]),
+    "ising_slab_set_stream": (I, [P, P]),
+    "ising_slab_set_table": (I, [P, P, I]),
+    "ising_slab_upload": (I, [P, P, P]),
+    "ising_slab_download": (I, [P, P, P]),
+    "ising_slab_fill_cold": (I, [P]),
+    "ising_slab_fill_philox": (I, [P, U64]),
+    "ising_slab_halo": (I, [P, I, I, ctypes.POINTER(P), PI64]),
+    "ising_slab_series_reset": (I, [P, I64]),
+    "ising_slab_half_sweep": (I, [P, I, U64, I64]),
+    "ising_slab_series_read": (I, [P, I64, P]),
+    "ising_slab_observables": (I, [P, PI64, PI64]),
+    "ising_slab_sync": (I, [P]),
     "ising_philox_rate": (I, [I, I, I, PD]),
     "ising_philox_range": (I, [I, U32, I64, U32, U32, U32, U32, U32, P]),
 }

@@ -1,0 +1,570 @@
+// Slab decomposition of one lattice over several devices (or several handles on one device).
+//
+// A slab handle owns a contiguous range [begin, begin + count) of the lattice's first axis: rows
+// y of a 2D lattice, planes z of a 3D one.  Its colour arrays hold the owned rows plus one halo
+// of the opposite side's neighbours on each side: one row (2D) or one plane of ly rows (3D),
+//
+//     [ low halo | owned rows 0 .. rows-1 | high halo ]     (rows `row_bytes` apart)
+//
+// A half-sweep of colour c reads only the opposite colour, so before it the caller copies the
+// opposite colour's boundary rows of the neighbouring slabs into this slab's halos (periodic
+// along the axis: the first slab's low halo is the last slab's last row or plane), over NCCL,
+// a peer copy or a local copy: ising_slab_halo gives the device addresses of the halos and of
+// the boundary rows to send.  The kernels never wrap along the slab axis: they read the halos.
+// Random numbers use the global site index (the local row plus the slab's first global row) and
+// the global row parity, so the slabs together are bit-identical to one handle holding the
+// whole lattice (src/pyising/philox.py:54-78 keys every site by its index, not by who owns it).
+// The (M, E) sums of a slab cover its owned sites; the lattice's are the sums over slabs.
+#include <cstring>
+
+#include "capi_internal.h"
+#include "int8_core.cuh"
+#include "msc_core.cuh"
+
+struct ising_slab {
+    int device = 0;
+    int ndim = 2;
+    int variant = ISING_VARIANT_INT8;
+    int algorithm = ISING_METROPOLIS;
+    int64_t shape[3] = {0, 0, 0};  // the whole lattice
+    int64_t begin = 0, count = 0;  // owned range of the first axis
+    long long rows = 0;            // owned rows: count (2D) or count * ly (3D)
+    long long halo = 0;            // rows per halo: 1 (2D) or ly (3D)
+    long long row0 = 0;            // global row index of owned row 0
+    int lh = 0, ly = 0, lz = 1;    // ly, lz: the local extents the kernels walk
+    int nw = 0, pitch = 0;
+    size_t row_bytes = 0;          // device bytes per row: pitch (int8) or 8 nw (msc)
+    size_t host_row = 0;           // host bytes per row: lh (int8) or 8 nw (msc)
+    uint64_t seed = 0;
+    uint32_t table[7] = {0, 0, 0, 0, 0, 0, 0};
+    int table_n = 5;
+    int rule = 0;
+    void* base[2] = {nullptr, nullptr};  // halo + rows + halo rows per colour
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    unsigned long long* d_acc = nullptr;  // (M, E) of ising_slab_observables
+    long long* d_series = nullptr;        // measured (M, E) pairs
+    int64_t series_cap = 0;
+    int sm_count = 148;
+    int max_blocks = 148 * 8;
+
+    char* owned(int c) const { return static_cast<char*>(base[c]) + halo * row_bytes; }
+};
+
+namespace ising {
+
+struct SlabGeo {
+    long long row0;  // global row of local row 0: the Philox site index is (row0 + row) * lh + j
+    int par0;        // parity of the slab's first global y (2D) or z (3D)
+};
+
+// int8 half-sweep of a slab: the band schedule of int8_half_kernel, with the rows next to the
+// slab (row -1 and row `rows` in 2D, planes -1 and lz in 3D) read from the halos instead of
+// wrapping.  Rows are 16-byte chunks with the partial-chunk code for padded rows.
+template <int NDIM, int RULE, bool MEAS>
+__global__ void __launch_bounds__(256, 4) int8_slab_kernel(const Int8Half p_in, const SlabGeo g)
+{
+    constexpr int V = 16, W = 4;
+    Int8Half p = p_in;
+    __shared__ u32 stab[8];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) stab[i] = p.table[i];
+    }
+    __syncthreads();
+    long long m_acc = 0, e_acc = 0;
+    const u32 cpr = (u32)p.cpr, bpp = (u32)p.bpp;
+    const u32 nslots = (u32)p.lz * bpp * cpr;
+    const int ly = p.ly;
+    for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
+         slot += gridDim.x * blockDim.x) {
+        const u32 band = fast_div(slot, cpr, p.cpr_magic);
+        const int j0 = (int)(slot - band * cpr) * V;
+        int z = 0, yb = (int)band;
+        if constexpr (NDIM == 3) {
+            z = (int)fast_div(band, bpp, p.bpp_magic);
+            yb = (int)(band - (u32)z * bpp);
+        }
+        const int y0 = yb * p.band;
+        const int y1 = y0 + p.band < ly ? y0 + p.band : ly;
+        const int wv = valid_words<true, W>(p, j0);
+        const long long plane = (long long)z * ly;
+        const int8_t* oth = p.other + j0;
+        // 2D: y is the slab axis, rows -1 and ly are halo rows; 3D: y wraps inside its plane
+        const long long yprev = NDIM == 2 ? y0 - 1 : (y0 == 0 ? ly - 1 : y0 - 1);
+        Words<W> nd = load_words_ro<W>(oth + (plane + yprev) * p.pitch);
+        Words<W> c = load_words_ro<W>(oth + (plane + y0) * p.pitch);
+        for (int y = y0; y < y1; ++y) {
+            const long long row = plane + y;
+            const long long ynext = NDIM == 2 ? y + 1 : (y + 1 == ly ? 0 : y + 1);
+            const Words<W> nu = load_words_ro<W>(oth + (plane + ynext) * p.pitch);
+            Words<W> zu = nu, zd = nd;
+            if constexpr (NDIM == 3) {  // planes z +- 1: plane -1 and plane lz are the halos
+                zu = load_words_ro<W>(oth + (row + ly) * p.pitch);
+                zd = load_words_ro<W>(oth + (row - ly) * p.pitch);
+            }
+            const int par = (g.par0 + y + z + (int)p.color) & 1;
+            const u32 edge =
+                (u32)(uint8_t)__ldg(p.other + row * p.pitch + edge_index(p, par, j0, wv));
+            const Words<W> s = load_words<W>(p.own + row * p.pitch + j0);
+            const Words<W> ns = int8_update<V, NDIM, RULE, true, MEAS, false>(
+                p, g.row0 + row, par, j0, wv, s, c, nu, nd, zu, zd, edge, stab, m_acc, e_acc);
+            if constexpr (RULE != kObserve) store_words<W>(p.own + row * p.pitch + j0, ns);
+            nd = c;
+            c = nu;
+        }
+    }
+    if constexpr (MEAS) block_accumulate2(m_acc, e_acc, p.meas);
+}
+
+// msc half-sweep of a 2D slab, one word per thread; rows -1 and `rows` are the halo rows.
+template <bool UPDATE, bool MEAS>
+__global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const SlabGeo g)
+{
+    long long m_acc = 0, e_acc = 0;
+    const int nw = p.nw;
+    const long long words = (long long)p.rows * nw;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < words;
+         w += (long long)gridDim.x * blockDim.x) {
+        const long long y = w / nw;
+        const int x = (int)(w - y * nw);
+        const long long rb = y * nw;
+        const u64* orow = p.other + rb;
+        const u64 o = p.own[rb + x];
+        const u64 c = __ldg(orow + x);
+        u64 hz;
+        if ((g.par0 + (int)(y & 1) + (int)p.color) & 1)
+            hz = (c >> 1) | (__ldg(orow + (x + 1 == nw ? 0 : x + 1)) << 63);
+        else hz = (c << 1) | (__ldg(orow + (x == 0 ? nw - 1 : x - 1)) >> 63);
+        const u64 up = __ldg(orow - nw + x);
+        const u64 dn = __ldg(orow + nw + x);
+        u64 ns = o;
+        if constexpr (UPDATE) {
+            const Slices s = slice4(o, c, hz, up, dn);
+            int calls = 0;
+            ns = o ^ msc_flip(s, (u32)((g.row0 + y) * nw + x), p.t, p.color, p.k0, p.k1, p.thr4,
+                              p.thr8, calls);
+            p.own[rb + x] = ns;
+        }
+        if constexpr (MEAS) {
+            const int anti =
+                __popcll(ns ^ c) + __popcll(ns ^ hz) + __popcll(ns ^ up) + __popcll(ns ^ dn);
+            m_acc += 2 * (__popcll(ns) + __popcll(c)) - 128;
+            e_acc += 2 * anti - 256;
+        }
+    }
+    if constexpr (MEAS) block_accumulate2(m_acc, e_acc, p.meas);
+}
+
+// The device seeded start of ising_fill_philox at global site indices.
+__global__ void slab_philox_int8_kernel(int8_t* c0, int8_t* c1, long long rows, long long row0,
+                                        int lh, int pitch, u32 k0, u32 k1)
+{
+    const int qpr = lh / 4;
+    const long long quads = rows * qpr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * quads;
+         i += (long long)gridDim.x * blockDim.x) {
+        const u32 color = (u32)(i / quads);
+        const long long qi = i - (long long)color * quads;
+        const long long row = qi / qpr;
+        const int q = (int)(qi - row * qpr);
+        const long long n = (row0 + row) * lh + 4LL * q;
+        const u32x4 r = philox4x32_10((u32)(n >> 7), 0u, color, 0xFFFFFFFFu, k0, k1);
+        const int word = (int)((n >> 5) & 3);
+        const u32 rw = word == 0 ? r.x : (word == 1 ? r.y : (word == 2 ? r.z : r.w));
+        const u32 nib = (rw >> (n & 31)) & 0xFu;
+        const u32 ones = (nib * 0x00204081u) & 0x01010101u;
+        *reinterpret_cast<u32*>((color ? c1 : c0) + row * pitch + 4 * q) =
+            0xFFFFFFFFu ^ (ones * 0xFEu);
+    }
+}
+
+__global__ void slab_philox_msc_kernel(u64* w0, u64* w1, long long rows, long long row0, int nw,
+                                       u32 k0, u32 k1)
+{
+    const long long words = rows * nw;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * words;
+         i += (long long)gridDim.x * blockDim.x) {
+        const u32 color = (u32)(i / words);
+        const long long wl = i - (long long)color * words;
+        const long long wg = row0 * nw + wl;  // global word index
+        const u32x4 r = philox4x32_10((u32)(wg >> 1), 0u, color, 0xFFFFFFFFu, k0, k1);
+        (color ? w1 : w0)[wl] =
+            (wg & 1) ? ((u64)r.z | ((u64)r.w << 32)) : ((u64)r.x | ((u64)r.y << 32));
+    }
+}
+
+static unsigned slab_grid(long long work, int max_blocks)
+{
+    long long g = (work + 255) / 256;
+    if (g > max_blocks) g = max_blocks;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <int NDIM, bool MEAS>
+static void launch_int8_slab_rule(int rule, const Int8Half& p, const SlabGeo& g, unsigned grid,
+                                  cudaStream_t st)
+{
+    switch (rule) {
+    case kMetroFast: int8_slab_kernel<NDIM, kMetroFast, MEAS><<<grid, 256, 0, st>>>(p, g); break;
+    case kHeatFast: int8_slab_kernel<NDIM, kHeatFast, MEAS><<<grid, 256, 0, st>>>(p, g); break;
+    case kMetroGeneric:
+        int8_slab_kernel<NDIM, kMetroGeneric, MEAS><<<grid, 256, 0, st>>>(p, g);
+        break;
+    case kHeatGeneric:
+        int8_slab_kernel<NDIM, kHeatGeneric, MEAS><<<grid, 256, 0, st>>>(p, g);
+        break;
+    default: int8_slab_kernel<NDIM, kObserve, true><<<grid, 256, 0, st>>>(p, g); break;
+    }
+}
+
+// One half-sweep of colour `color` (rule kObserve: measurement of colour `color` only).
+static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long long* meas)
+{
+    const SlabGeo g{s->row0, (int)(s->begin & 1)};
+    if (s->variant == ISING_VARIANT_MSC) {
+        MscHalf p;
+        memset(&p, 0, sizeof p);
+        p.own = reinterpret_cast<u64*>(s->owned(color));
+        p.other = reinterpret_cast<const u64*>(s->owned(1 - color));
+        p.rows = (int)s->rows;
+        p.nw = s->nw;
+        p.t = t;
+        p.color = (u32)color;
+        p.k0 = (u32)s->seed;
+        p.k1 = (u32)(s->seed >> 32);
+        p.thr4 = s->table[3];
+        p.thr8 = s->table[4];
+        p.meas = meas;
+        const unsigned grid = slab_grid(s->rows * (long long)s->nw, s->max_blocks);
+        if (rule == kObserve) msc_slab_kernel<false, true><<<grid, 256, 0, s->stream>>>(p, g);
+        else if (meas) msc_slab_kernel<true, true><<<grid, 256, 0, s->stream>>>(p, g);
+        else msc_slab_kernel<true, false><<<grid, 256, 0, s->stream>>>(p, g);
+    } else {
+        Int8Half p;
+        memset(&p, 0, sizeof p);
+        p.own = reinterpret_cast<int8_t*>(s->owned(color));
+        p.other = reinterpret_cast<const int8_t*>(s->owned(1 - color));
+        p.rows = s->rows;
+        p.lh = s->lh;
+        p.ly = s->ly;
+        p.lz = s->lz;
+        p.pitch = s->pitch;
+        p.vw = 16;
+        p.cpr = (s->lh + 15) / 16;
+        p.t = t;
+        p.color = (u32)color;
+        p.k0 = (u32)s->seed;
+        p.k1 = (u32)(s->seed >> 32);
+        for (int i = 0; i < 7; ++i) p.table[i] = s->table[i];
+        p.meas = meas;
+        const unsigned grid = int8_band_geometry(p, s->max_blocks, s->sm_count);
+        const bool m = meas != nullptr;
+        if (s->ndim == 3) {
+            if (m) launch_int8_slab_rule<3, true>(rule, p, g, grid, s->stream);
+            else launch_int8_slab_rule<3, false>(rule, p, g, grid, s->stream);
+        } else {
+            if (m) launch_int8_slab_rule<2, true>(rule, p, g, grid, s->stream);
+            else launch_int8_slab_rule<2, false>(rule, p, g, grid, s->stream);
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
+}
+
+}  // namespace ising
+
+using namespace ising;
+
+#define SLAB_TRY(call)                                       \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+    } while (0)
+
+#define SLAB_CHECK(s)                                                   \
+    do {                                                                \
+        if (!(s)) return fail(ISING_ERR_INVALID, "null slab handle");  \
+    } while (0)
+
+extern "C" {
+
+int ising_slab_create(int ndim, const int64_t* shape, int variant, int algorithm, uint64_t seed,
+                      int64_t begin, int64_t count, int device, ising_slab** out)
+{
+    if (!out || !shape) return fail(ISING_ERR_INVALID, "null pointer argument");
+    *out = nullptr;
+    if (ndim != 2 && ndim != 3)
+        return fail(ISING_ERR_INVALID, "only 2D and 3D lattices are supported, got ndim=%d", ndim);
+    for (int i = 0; i < ndim; ++i)
+        if (shape[i] < 2 || shape[i] % 2)
+            return fail(ISING_ERR_INVALID, "all extents must be even and >= 2");
+    if (variant != ISING_VARIANT_INT8 && variant != ISING_VARIANT_MSC)
+        return fail(ISING_ERR_INVALID, "unknown variant %d", variant);
+    if (algorithm != ISING_METROPOLIS && algorithm != ISING_HEATBATH)
+        return fail(ISING_ERR_INVALID, "unknown algorithm %d", algorithm);
+    const int64_t lx = shape[ndim - 1];
+    const int multiple = variant == ISING_VARIANT_MSC ? 128 : 8;
+    if (lx % multiple)
+        return fail(ISING_ERR_INVALID, "last extent must be a multiple of %d, got %lld", multiple,
+                    (long long)lx);
+    if (variant == ISING_VARIANT_MSC && (ndim != 2 || algorithm != ISING_METROPOLIS))
+        return fail(ISING_ERR_INVALID, "msc supports 2D Metropolis only");
+    const int64_t ly = shape[ndim - 2];
+    const int64_t lz = ndim == 3 ? shape[0] : 1;
+    if (ly * lz > (int64_t)0x7FFFFFFF || lx / 2 > (int64_t)0x7FFFFFFF)
+        return fail(ISING_ERR_INVALID, "lattice too large for 32-bit row indices");
+    if (count < 1 || begin < 0 || begin + count > shape[0])
+        return fail(ISING_ERR_INVALID, "slab [%lld, %lld) outside the first axis (extent %lld)",
+                    (long long)begin, (long long)(begin + count), (long long)shape[0]);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(ISING_ERR_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev)
+        return fail(ISING_ERR_INVALID, "device %d out of range (%d devices)", device, ndev);
+    SLAB_TRY(cudaSetDevice(device));
+
+    ising_slab* s = new ising_slab();
+    s->device = device;
+    s->ndim = ndim;
+    s->variant = variant;
+    s->algorithm = algorithm;
+    for (int i = 0; i < 3; ++i) s->shape[i] = i < ndim ? shape[i] : 0;
+    s->begin = begin;
+    s->count = count;
+    s->lh = (int)(lx / 2);
+    s->nw = (int)(lx / 128);
+    s->pitch = (s->lh + 15) / 16 * 16;
+    if (ndim == 2) {
+        s->ly = (int)count;  // the kernels walk the owned rows as one plane
+        s->lz = 1;
+        s->halo = 1;
+        s->row0 = begin;
+    } else {
+        s->ly = (int)ly;
+        s->lz = (int)count;
+        s->halo = ly;
+        s->row0 = begin * ly;
+    }
+    s->rows = (long long)s->ly * s->lz;
+    s->row_bytes = variant == ISING_VARIANT_MSC ? (size_t)s->nw * 8 : (size_t)s->pitch;
+    s->host_row = variant == ISING_VARIANT_MSC ? (size_t)s->nw * 8 : (size_t)s->lh;
+    s->seed = seed;
+    s->table_n = 2 * ndim + 1;
+    for (int i = 0; i < 7; ++i) s->table[i] = 0xFFFFFFFFu;
+    s->rule = select_rule(variant, algorithm, ndim, s->table);
+    s->sm_count = device_sm_count(device);
+    s->max_blocks = s->sm_count * 8;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    s->stream = s->own_stream;
+    const size_t bytes = (size_t)(s->rows + 2 * s->halo) * s->row_bytes;
+    for (int c = 0; c < 2; ++c) {
+        e = cudaMalloc(&s->base[c], bytes);
+        if (e == cudaSuccess) e = cudaMemset(s->base[c], 0, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ising_slab_destroy(s);
+            return fail(ISING_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", bytes,
+                        cudaGetErrorString(e));
+        }
+    }
+    e = cudaMalloc(&s->d_acc, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ising_slab_destroy(s);
+        return fail(ISING_ERR_NOMEM, "cudaMalloc of the accumulators failed");
+    }
+    *out = s;
+    return ISING_OK;
+}
+
+int ising_slab_destroy(ising_slab* s)
+{
+    if (!s) return ISING_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (int c = 0; c < 2; ++c)
+        if (s->base[c]) cudaFree(s->base[c]);
+    if (s->d_acc) cudaFree(s->d_acc);
+    if (s->d_series) cudaFree(s->d_series);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    cudaGetLastError();
+    delete s;
+    return ISING_OK;
+}
+
+int ising_slab_set_stream(ising_slab* s, void* stream)
+{
+    SLAB_CHECK(s);
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return ISING_OK;
+}
+
+int ising_slab_set_table(ising_slab* s, const uint32_t* table, int n)
+{
+    SLAB_CHECK(s);
+    if (!table) return fail(ISING_ERR_INVALID, "null table");
+    if (n != s->table_n)
+        return fail(ISING_ERR_INVALID, "table must have %d entries, got %d", s->table_n, n);
+    for (int i = 0; i < 7; ++i) s->table[i] = i < n ? table[i] : 0xFFFFFFFFu;
+    s->rule = select_rule(s->variant, s->algorithm, s->ndim, s->table);
+    return ISING_OK;
+}
+
+int ising_slab_upload(ising_slab* s, const void* c0, const void* c1)
+{
+    SLAB_CHECK(s);
+    if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
+    SLAB_TRY(cudaSetDevice(s->device));
+    const void* src[2] = {c0, c1};
+    for (int c = 0; c < 2; ++c)
+        SLAB_TRY(cudaMemcpy2DAsync(s->owned(c), s->row_bytes, src[c], s->host_row, s->host_row,
+                                   (size_t)s->rows, cudaMemcpyHostToDevice, s->stream));
+    SLAB_TRY(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+int ising_slab_download(ising_slab* s, void* c0, void* c1)
+{
+    SLAB_CHECK(s);
+    if (!c0 || !c1) return fail(ISING_ERR_INVALID, "null colour array");
+    SLAB_TRY(cudaSetDevice(s->device));
+    void* dst[2] = {c0, c1};
+    for (int c = 0; c < 2; ++c)
+        SLAB_TRY(cudaMemcpy2DAsync(dst[c], s->host_row, s->owned(c), s->row_bytes, s->host_row,
+                                   (size_t)s->rows, cudaMemcpyDeviceToHost, s->stream));
+    SLAB_TRY(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+int ising_slab_fill_cold(ising_slab* s)
+{
+    SLAB_CHECK(s);
+    SLAB_TRY(cudaSetDevice(s->device));
+    const int v = s->variant == ISING_VARIANT_MSC ? 0xFF : 0x01;
+    const size_t bytes = (size_t)(s->rows + 2 * s->halo) * s->row_bytes;
+    for (int c = 0; c < 2; ++c) SLAB_TRY(cudaMemsetAsync(s->base[c], v, bytes, s->stream));
+    return ISING_OK;
+}
+
+int ising_slab_fill_philox(ising_slab* s, uint64_t start_seed)
+{
+    SLAB_CHECK(s);
+    SLAB_TRY(cudaSetDevice(s->device));
+    const u32 k0 = (u32)start_seed, k1 = (u32)(start_seed >> 32);
+    if (s->variant == ISING_VARIANT_MSC) {
+        slab_philox_msc_kernel<<<slab_grid(2 * s->rows * s->nw, s->max_blocks), 256, 0,
+                                 s->stream>>>(reinterpret_cast<u64*>(s->owned(0)),
+                                              reinterpret_cast<u64*>(s->owned(1)), s->rows,
+                                              s->row0, s->nw, k0, k1);
+    } else {
+        slab_philox_int8_kernel<<<slab_grid(2 * s->rows * (s->lh / 4), s->max_blocks), 256, 0,
+                                  s->stream>>>(reinterpret_cast<int8_t*>(s->owned(0)),
+                                               reinterpret_cast<int8_t*>(s->owned(1)), s->rows,
+                                               s->row0, s->lh, s->pitch, k0, k1);
+    }
+    SLAB_TRY(cudaGetLastError());
+    return ISING_OK;
+}
+
+int ising_slab_halo(ising_slab* s, int color, int which, void** ptr, int64_t* bytes)
+{
+    SLAB_CHECK(s);
+    if (!ptr || !bytes) return fail(ISING_ERR_INVALID, "null output pointer");
+    if (color != 0 && color != 1) return fail(ISING_ERR_INVALID, "colour must be 0 or 1");
+    char* own = s->owned(color);
+    const long long hb = s->halo * (long long)s->row_bytes;
+    switch (which) {
+    case ISING_SLAB_HALO_LOW: *ptr = own - hb; break;
+    case ISING_SLAB_HALO_HIGH: *ptr = own + s->rows * (long long)s->row_bytes; break;
+    case ISING_SLAB_EDGE_LOW: *ptr = own; break;
+    case ISING_SLAB_EDGE_HIGH: *ptr = own + (s->rows - s->halo) * (long long)s->row_bytes; break;
+    default: return fail(ISING_ERR_INVALID, "unknown halo selector %d", which);
+    }
+    *bytes = hb;
+    return ISING_OK;
+}
+
+int ising_slab_series_reset(ising_slab* s, int64_t pairs)
+{
+    SLAB_CHECK(s);
+    if (pairs < 0) return fail(ISING_ERR_INVALID, "negative series length");
+    SLAB_TRY(cudaSetDevice(s->device));
+    if (pairs > s->series_cap) {
+        if (s->d_series) {
+            SLAB_TRY(cudaStreamSynchronize(s->stream));
+            cudaFree(s->d_series);
+            s->d_series = nullptr;
+            s->series_cap = 0;
+        }
+        cudaError_t e = cudaMalloc((void**)&s->d_series, (size_t)pairs * 2 * sizeof(long long));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ISING_ERR_NOMEM, "cudaMalloc of a series of %lld pairs", (long long)pairs);
+        }
+        s->series_cap = pairs;
+    }
+    if (pairs > 0)
+        SLAB_TRY(cudaMemsetAsync(s->d_series, 0, (size_t)pairs * 2 * sizeof(long long), s->stream));
+    return ISING_OK;
+}
+
+int ising_slab_half_sweep(ising_slab* s, int color, uint64_t t, int64_t slot)
+{
+    SLAB_CHECK(s);
+    if (color != 0 && color != 1) return fail(ISING_ERR_INVALID, "colour must be 0 or 1");
+    if (slot >= s->series_cap)
+        return fail(ISING_ERR_INVALID, "series slot %lld beyond the %lld reset pairs",
+                    (long long)slot, (long long)s->series_cap);
+    SLAB_TRY(cudaSetDevice(s->device));
+    unsigned long long* m =
+        slot >= 0 ? reinterpret_cast<unsigned long long*>(s->d_series + 2 * slot) : nullptr;
+    return slab_half(s, color, (u32)t, s->rule, m);
+}
+
+int ising_slab_series_read(ising_slab* s, int64_t pairs, int64_t* out)
+{
+    SLAB_CHECK(s);
+    if (pairs < 0 || pairs > s->series_cap)
+        return fail(ISING_ERR_INVALID, "series of %lld pairs, %lld reset", (long long)pairs,
+                    (long long)s->series_cap);
+    if (pairs > 0 && !out) return fail(ISING_ERR_INVALID, "null output pointer");
+    SLAB_TRY(cudaSetDevice(s->device));
+    if (pairs > 0)
+        SLAB_TRY(cudaMemcpyAsync(out, s->d_series, (size_t)pairs * 2 * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, s->stream));
+    SLAB_TRY(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+int ising_slab_observables(ising_slab* s, int64_t* m, int64_t* e)
+{
+    SLAB_CHECK(s);
+    if (!m || !e) return fail(ISING_ERR_INVALID, "null output pointer");
+    SLAB_TRY(cudaSetDevice(s->device));
+    SLAB_TRY(cudaMemsetAsync(s->d_acc, 0, 2 * sizeof(unsigned long long), s->stream));
+    const int rc = slab_half(s, 1, 0u, kObserve, s->d_acc);
+    if (rc != ISING_OK) return rc;
+    long long out[2];
+    SLAB_TRY(cudaMemcpyAsync(out, s->d_acc, sizeof out, cudaMemcpyDeviceToHost, s->stream));
+    SLAB_TRY(cudaStreamSynchronize(s->stream));
+    *m = out[0];
+    *e = out[1];
+    return ISING_OK;
+}
+
+int ising_slab_sync(ising_slab* s)
+{
+    SLAB_CHECK(s);
+    SLAB_TRY(cudaSetDevice(s->device));
+    SLAB_TRY(cudaStreamSynchronize(s->stream));
+    return ISING_OK;
+}
+
+}  // extern "C"

@@ -19,7 +19,10 @@
 
 namespace ising {
 
-constexpr int kTbBand = 8;                       // rows a CTA writes back
+#ifndef ISING_TB_BAND
+#define ISING_TB_BAND 8
+#endif
+constexpr int kTbBand = ISING_TB_BAND;           // rows a CTA writes back
 constexpr int kTbSteps = 4;                      // half-sweeps per launch: two sweeps
 constexpr int kTbRows = kTbBand + 2 * kTbSteps;  // tile rows per colour
 constexpr int kTbMaxSmem = 96 * 1024;

@@ -60,3 +60,44 @@ def random_lattice(shape, seed: int) -> np.ndarray:
     (src/pyising/lattice.py:93-96), so hot starts match pyising's NumPy backend exactly."""
     rng = np.random.default_rng(seed)
     return (rng.integers(0, 2, size=tuple(shape), dtype=np.int8) * 2 - 1).astype(np.int8)
+
+
+def row_parity(shape) -> np.ndarray:
+    """Parity of the sum of the non-x indices of every row, rows in C order
+    (src/pyising/lattice.py:43-47)."""
+    return (np.indices(tuple(shape[:-1])).sum(axis=0) & 1).reshape(-1)
+
+
+def split_colours(lat: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The two compressed colour arrays (rows, Lx/2) of a full lattice on the host: colour c of
+    a row of parity p sits at x = 2j + ((p + c) % 2) (src/pyising/lattice.py:50-61)."""
+    flat = np.asarray(lat).reshape(-1, lat.shape[-1])
+    odd = (row_parity(lat.shape) == 1)[:, None]
+    even_x, odd_x = flat[:, 0::2], flat[:, 1::2]
+    return (np.ascontiguousarray(np.where(odd, odd_x, even_x)),
+            np.ascontiguousarray(np.where(odd, even_x, odd_x)))
+
+
+def merge_colours(c0: np.ndarray, c1: np.ndarray, shape) -> np.ndarray:
+    """The full lattice from its two compressed colour arrays (src/pyising/lattice.py:64-72)."""
+    shape = tuple(shape)
+    odd = (row_parity(shape) == 1)[:, None]
+    flat = np.empty((c0.shape[0], shape[-1]), dtype=np.int8)
+    flat[:, 0::2] = np.where(odd, c1, c0)
+    flat[:, 1::2] = np.where(odd, c0, c1)
+    return flat.reshape(shape)
+
+
+def pack_colour(comp: np.ndarray) -> np.ndarray:
+    """Packed words (rows, Lh/64) of a compressed colour array: bit b of word w is site 64w + b,
+    set for +1 (src/pyising/lattice.py:75-82)."""
+    rows, lh = comp.shape
+    bits = (np.asarray(comp) > 0).reshape(rows, lh // 64, 64)
+    return np.packbits(bits, axis=2, bitorder="little").view("<u8").reshape(rows, lh // 64)
+
+
+def unpack_colour(words: np.ndarray) -> np.ndarray:
+    """The compressed int8 colour array of packed words (src/pyising/lattice.py:85-90)."""
+    rows, nw = words.shape
+    bytes_ = np.ascontiguousarray(words).view(np.uint8).reshape(rows, 8 * nw)
+    return np.unpackbits(bytes_, axis=1, bitorder="little").astype(np.int8) * 2 - 1

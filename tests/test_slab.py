@@ -1,0 +1,277 @@
+"""Slab decomposition of one lattice (pyising_b200.slab).
+
+CPU: the sweep loop (SlabRunner) and both halo exchanges run on CPU slabs whose half-sweep is
+a NumPy restatement of the reference update (src/pyising/backends/numpy_backend.py:26-44)
+working only on the slab's rows and halos: in one process (LocalExchange) and as gloo ranks of
+world size 2 (RingExchange, the code path NCCL runs on GPUs).  Spins and (M, E) series must be
+bit-identical to the oracle running the whole lattice.
+
+GPU: the C-ABI slab handles (ising_slab_*) split over several slabs on one GPU must be
+bit-identical to one handle holding the whole lattice, for int8 2D/3D (Metropolis, heat bath)
+and msc, uneven slabs included.
+"""
+
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+import oracle
+from pyising_b200.slab import (EDGE_HIGH, EDGE_LOW, HALO_HIGH, HALO_LOW, LocalExchange,
+                               RingExchange, SlabRunner, partition)
+
+
+def test_partition_covers_the_axis():
+    for extent in (2, 7, 16, 33):
+        for parts in range(1, min(extent, 6) + 1):
+            ranges = partition(extent, parts)
+            assert ranges[0][0] == 0 and sum(c for _, c in ranges) == extent
+            assert all(b1 == b0 + c0 for (b0, c0), (b1, _) in zip(ranges, ranges[1:]))
+            assert max(c for _, c in ranges) - min(c for _, c in ranges) <= 1
+    with pytest.raises(ValueError):
+        partition(4, 5)
+    with pytest.raises(ValueError):
+        partition(4, 0)
+
+
+class CpuSlab:
+    """A slab of an int8 lattice on the CPU with the C-ABI slab's interface: rows
+    [begin, begin + count) of the first axis plus one halo row (2D) or plane (3D) per side,
+    updated from its own rows and halos only."""
+
+    def __init__(self, lat, begin, count, beta, seed, algorithm):
+        shape = lat.shape
+        self.ndim = len(shape)
+        self.ly = shape[1] if self.ndim == 3 else count
+        inner = shape[1] if self.ndim == 3 else 1
+        self.rows, self.row0 = count * inner, begin * inner
+        self.halo = inner
+        self.par0 = begin & 1
+        self.lh = shape[-1] // 2
+        self.k0, self.k1 = oracle.split_seed(seed)
+        self.table = oracle.threshold_table(beta, self.ndim, algorithm)
+        self.heat = algorithm == "heatbath"
+        full = oracle.to_compressed(lat)
+        self.a = []
+        for c in (0, 1):
+            arr = np.zeros((self.rows + 2 * self.halo, self.lh), np.int8)
+            arr[self.halo:self.halo + self.rows] = full[c][self.row0:self.row0 + self.rows]
+            self.a.append(arr)
+        self.series = np.zeros((0, 2), np.int64)
+
+    def region(self, colour, which):
+        h, r, arr = self.halo, self.rows, self.a[colour]
+        sl = {HALO_LOW: slice(0, h), HALO_HIGH: slice(h + r, 2 * h + r),
+              EDGE_LOW: slice(h, 2 * h), EDGE_HIGH: slice(r, h + r)}[which]
+        return torch.from_numpy(arr[sl].reshape(-1).view(np.uint8))
+
+    def _field(self, colour):
+        """Sum of the opposite colour's neighbours of every owned site of `colour`."""
+        h, rows, ly, lh = self.halo, self.rows, self.ly, self.lh
+        oth = self.a[1 - colour].astype(np.int64)
+        r = np.arange(rows)
+        z, y = (r // ly, r % ly) if self.ndim == 3 else (np.zeros_like(r), r)
+        same = oth[h + r]
+        par = ((self.par0 + y + z + colour) & 1)[:, None]
+        field = same + np.where(par == 1, np.roll(same, -1, axis=1), np.roll(same, 1, axis=1))
+        if self.ndim == 2:
+            field += oth[h + r - 1] + oth[h + r + 1]
+        else:
+            plane = z * ly
+            field += oth[h + plane + (y + 1) % ly] + oth[h + plane + (y - 1) % ly]
+            field += oth[h + r + ly] + oth[h + r - ly]
+        return field
+
+    def half_sweep(self, colour, t, slot=-1):
+        own = self.a[colour][self.halo:self.halo + self.rows]
+        field = self._field(colour)
+        q0, n = self.row0 * self.lh // 4, self.rows * self.lh // 4
+        u = oracle.philox_range(q0, n, t, colour, 0, self.k0, self.k1).reshape(own.shape)
+        d = 2 * self.ndim
+        if self.heat:
+            own[:] = np.where(u < self.table[(field + d) // 2], 1, -1)
+        else:
+            x = own * field
+            flip = (x <= 0) | (u < self.table[(x + d) // 2])
+            own[:] = np.where(flip, -own, own)
+        if slot >= 0:
+            self.series[slot] += self.observables()
+
+    def observables(self):
+        h, r = self.halo, self.rows
+        s1 = self.a[1][h:h + r].astype(np.int64)
+        m = int(s1.sum() + self.a[0][h:h + r].astype(np.int64).sum())
+        return m, -int((s1 * self._field(1)).sum())
+
+    def series_reset(self, pairs):
+        self.series = np.zeros((pairs, 2), np.int64)
+
+    def series_read(self, pairs):
+        return self.series[:pairs].copy()
+
+    def compressed(self):
+        return [x[self.halo:self.halo + self.rows] for x in self.a]
+
+
+CASES = [((10, 16), 0.44, "metropolis", 12345, 3),
+         ((6, 4, 8), 0.22, "heatbath", 7, 2),
+         ((8, 6, 16), 0.3, "metropolis", 2**40 + 1, 4),
+         ((14, 24), 0.6, "heatbath", 99, 5)]
+
+
+def _oracle_run(shape, beta, algorithm, seed, sweeps, every):
+    lat = oracle.random_lattice(shape, seed)
+    sim = oracle.OracleInt8(shape, beta, seed=seed, algorithm=algorithm, init=lat)
+    series = sim.sweep(sweeps, measure_every=every)
+    return lat, series, sim.get_lattice(), sim.observables_int()
+
+
+def _assemble(shape, slabs):
+    c0 = np.concatenate([s.compressed()[0] for s in slabs])
+    c1 = np.concatenate([s.compressed()[1] for s in slabs])
+    return oracle.from_compressed(c0, c1, shape)
+
+
+@pytest.mark.parametrize("shape,beta,algorithm,seed,parts", CASES)
+def test_local_exchange_matches_whole_lattice(shape, beta, algorithm, seed, parts):
+    lat, series, final, obs = _oracle_run(shape, beta, algorithm, seed, 6, 2)
+    slabs = [CpuSlab(lat, b, c, beta, seed, algorithm) for b, c in partition(shape[0], parts)]
+    runner = SlabRunner(slabs, LocalExchange())
+    got = runner.sweep(6, 2)
+    np.testing.assert_array_equal(got, series)
+    np.testing.assert_array_equal(_assemble(shape, slabs), final)
+    assert runner.observables_int() == obs
+    assert runner.t == 6
+
+
+def _ring_worker(rank, world, port, queue):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out = []
+        for shape, beta, algorithm, seed, _ in CASES:
+            lat = oracle.random_lattice(shape, seed)
+            b, c = partition(shape[0], world)[rank]
+            slab = CpuSlab(lat, b, c, beta, seed, algorithm)
+            runner = SlabRunner([slab], RingExchange(None, device="cpu"))
+            series = runner.sweep(5, 1)
+            runner.sweep(2)
+            obs = runner.observables_int()
+            out.append((series, b, slab.compressed(), obs))
+        queue.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_ring_exchange_world2_gloo():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ring_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=180) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for k, (shape, beta, algorithm, seed, _) in enumerate(CASES):
+        lat = oracle.random_lattice(shape, seed)
+        sim = oracle.OracleInt8(shape, beta, seed=seed, algorithm=algorithm, init=lat)
+        want_series = sim.sweep(5, measure_every=1)
+        sim.sweep(2)
+        for rank in (0, 1):
+            series, _, _, obs = got[rank][k]
+            np.testing.assert_array_equal(series, want_series)
+            assert obs == sim.observables_int()
+        parts = sorted((got[r][k][1], got[r][k][2]) for r in (0, 1))
+        c0 = np.concatenate([p[1][0] for p in parts])
+        c1 = np.concatenate([p[1][1] for p in parts])
+        np.testing.assert_array_equal(oracle.from_compressed(c0, c1, shape), sim.get_lattice())
+
+
+# ------------------------------------------------------------------------------ GPU ---------
+GPU_CASES = [
+    ("int8", (64, 96), "metropolis", 0.44, 2),
+    ("int8", (30, 48), "heatbath", 0.5, 3),   # uneven slabs, odd first rows
+    ("int8", (12, 10, 40), "metropolis", 0.22, 3),
+    ("int8", (10, 8, 32), "heatbath", 0.25, 4),
+    ("msc", (34, 256), "metropolis", 0.44, 3),
+    ("int8", (32, 64), "heatbath", -0.3, 2),  # negative beta: the per-site lookup rule
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant,shape,algorithm,beta,parts", GPU_CASES)
+def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts):
+    from pyising_b200.backend import B200Int8, B200MultiSpin
+    from pyising_b200.slab import SlabSimulation
+
+    seed = 2024
+    one_cls = B200MultiSpin if variant == "msc" else B200Int8
+    one = one_cls(shape, beta, seed=seed, algorithm=algorithm, init="hot")
+    split = SlabSimulation(shape, beta, seed=seed, algorithm=algorithm, variant=variant,
+                           init="hot", parts=parts, devices=[0])
+    np.testing.assert_array_equal(split.get_lattice(), one.get_lattice())
+    want = one.sweep_measured(12, 3)
+    got = split.sweep_measured(12, 3)
+    np.testing.assert_array_equal(got, want)
+    one.sweep(5)
+    split.sweep(5)
+    assert split.t == one.t == 17
+    np.testing.assert_array_equal(split.get_lattice(), one.get_lattice())
+    assert split.observables_int() == one.observables_int()
+    split.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant,shape", [("int8", (24, 40)), ("int8", (6, 8, 16)),
+                                           ("msc", (20, 128))])
+def test_gpu_slab_philox_start_and_oracle(variant, shape):
+    from pyising_b200.slab import SlabSimulation
+
+    split = SlabSimulation(shape, 0.4 if len(shape) == 2 else 0.2, seed=77, variant=variant,
+                           init="philox", parts=3, devices=[0])
+    lat = oracle.philox_start(shape, 77)
+    np.testing.assert_array_equal(split.get_lattice(), lat)
+    sim = oracle.create(variant, shape=shape, beta=split.beta, seed=77, init=lat)
+    np.testing.assert_array_equal(split.sweep_measured(4, 2), sim.sweep(4, measure_every=2))
+    np.testing.assert_array_equal(split.get_lattice(), sim.get_lattice())
+    split.set_beta(0.1)
+    sim.set_beta(0.1)
+    split.sweep(3)
+    sim.sweep(3)
+    np.testing.assert_array_equal(split.get_lattice(), sim.get_lattice())
+    split.close()
+
+
+@pytest.mark.gpu
+def test_gpu_slab_argument_errors():
+    from pyising_b200.slab import Slab
+
+    tab = oracle.threshold_table(0.4, 2, "metropolis")
+    with pytest.raises(ValueError):
+        Slab((16, 16), tab, 0, "metropolis", "int8", 10, 8)  # beyond the axis
+    with pytest.raises(ValueError):
+        Slab((16, 16), tab, 0, "metropolis", "int8", 0, 0)
+    with pytest.raises(ValueError):
+        Slab((16, 16, 16), tab, 0, "metropolis", "msc", 0, 4)
+    s = Slab((16, 16), tab, 0, "metropolis", "int8", 4, 4)
+    with pytest.raises(ValueError):
+        s.half_sweep(0, 0, slot=0)  # no series reset
+    with pytest.raises(ValueError):
+        s.half_sweep(2, 0)
+    s.close()
