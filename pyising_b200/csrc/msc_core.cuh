@@ -155,14 +155,24 @@ __device__ __forceinline__ void call_levels(const u32x4& r, const uint4& m, u32 
     level32(r.w, m.z, m.w, a1h, undh, resh);
 }
 
+// Where a lattice piece sits in a bigger lattice (slab decomposition): the Philox word index is
+// w0 + the local word index and the row parity that of the global row (par0 + local row); rows
+// -1 and `rows` are halo rows, not wrapped.  Unused (and compiled out) for whole lattices.
+struct SlabOffset {
+    long long w0;
+    int par0;
+};
+
 // Global words of one intake batch (one per lane), loaded ahead of use.
 struct IntakeLoads {
     u64 o, c, side, up, dn;
     int y;  // row of the word
 };
 
+template <bool SLAB = false>
 __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool valid, int nw,
-                                            int nw_shift, IntakeLoads& L)
+                                            int nw_shift, IntakeLoads& L,
+                                            const SlabOffset& so = SlabOffset{0, 0})
 {
     if (!valid) {
         L.o = L.c = L.side = L.up = L.dn = 0;
@@ -181,18 +191,27 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
     const u64* orow = p.other + (long long)y * nw;
     L.o = p.own[w];
     L.c = __ldg(orow + x);
-    const int xs = ((y + (int)p.color) & 1) ? (x + 1 == nw ? 0 : x + 1) : (x == 0 ? nw - 1 : x - 1);
+    const int py = SLAB ? y + so.par0 : y;
+    const int xs = ((py + (int)p.color) & 1) ? (x + 1 == nw ? 0 : x + 1) : (x == 0 ? nw - 1 : x - 1);
     L.side = __ldg(orow + xs);
-    L.up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
-    L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
+    if constexpr (SLAB) {
+        L.up = __ldg(orow - nw + x);  // row -1 is the low halo
+        L.dn = __ldg(orow + nw + x);  // row `rows` is the high halo
+    } else {
+        L.up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
+        L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
+    }
 }
 
 // The whole warp updates words [begin, end) of the lattice in p.  `lvmask` holds
 // level_masks(p.thr4, p.thr8, lp) for lp = 0..15; `q` is this warp's stack.
+template <bool SLAB = false>
 __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begin, long long end,
                                                 int nw_shift, QueueSlots& q,
-                                                const uint4* lvmask)
+                                                const uint4* lvmask,
+                                                const SlabOffset& so = SlabOffset{0, 0})
 {
+    const u32 wg = SLAB ? (u32)so.w0 : 0u;  // Philox word index = wg + local index (mod 2^32)
     const int lane = threadIdx.x & 31;
     const u32 lt = (1u << lane) - 1u;
     const int nw = p.nw;
@@ -201,13 +220,13 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
     IntakeLoads L;
     long long w = next + lane;
     bool more = next < end;
-    if (more) intake_load(p, w, w < end, nw, nw_shift, L);
+    if (more) intake_load<SLAB>(p, w, w < end, nw, nw_shift, L, so);
     while (true) {
         if (n < kPop && more) {
             const bool valid = w < end;
             u32 a1l = 0, a1h = 0, undl = 0, undh = 0, resl = 0, resh = 0;
             if (valid) {
-                const bool par = (L.y + (int)p.color) & 1;
+                const bool par = ((SLAB ? L.y + so.par0 : L.y) + (int)p.color) & 1;
                 const u64 hz = par ? ((L.c >> 1) | (L.side << 63)) : ((L.c << 1) | (L.side >> 63));
                 const Slices s = slice4(L.o, L.c, hz, L.up, L.dn);
                 a1l = (u32)s.a1;
@@ -222,11 +241,12 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             next += 32;
             more = next < end;
             w = next + lane;
-            if (more) intake_load(p, w, w < end, nw, nw_shift, L);
+            if (more) intake_load<SLAB>(p, w, w < end, nw, nw_shift, L, so);
             if (valid) {
 #pragma unroll
                 for (int c3 = 0; c3 < kIntakeCalls; ++c3) {
-                    const u32x4 r = philox4x32_10((u32)wc, p.t, p.color, 1u + (u32)c3, p.k0, p.k1);
+                    const u32x4 r =
+                        philox4x32_10(wg + (u32)wc, p.t, p.color, 1u + (u32)c3, p.k0, p.k1);
                     call_levels(r, lvmask[c3], a1l, a1h, undl, undh, resl, resh);
                 }
             }
@@ -268,7 +288,8 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
 #pragma unroll
             for (int m = 0; m < ISING_MSC_POP; ++m) {
                 if (act[m]) {
-                    const u32x4 r = philox4x32_10(idx[m], p.t, p.color, 1u + lp[m], p.k0, p.k1);
+                    const u32x4 r =
+                        philox4x32_10(wg + idx[m], p.t, p.color, 1u + lp[m], p.k0, p.k1);
                     call_levels(r, lvmask[lp[m]], (u32)a1[m], (u32)(a1[m] >> 32), undl[m],
                                 undh[m], resl[m], resh[m]);
                     ++lp[m];

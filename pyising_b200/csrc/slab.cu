@@ -47,6 +47,7 @@ struct ising_slab {
     int64_t series_cap = 0;
     int sm_count = 148;
     int max_blocks = 148 * 8;
+    int queue_blocks = 2;  // resident blocks per SM of the msc work-stack kernel
 
     char* owned(int c) const { return static_cast<char*>(base[c]) + halo * row_bytes; }
 };
@@ -156,6 +157,38 @@ __global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const Sl
     if constexpr (MEAS) block_accumulate2(m_acc, e_acc, p.meas);
 }
 
+// Unmeasured msc half-sweep of a slab on the work stack of msc_half_queue_kernel: each warp walks
+// a contiguous range of the slab's words, with global Philox word indices and halo rows.
+constexpr int kSlabQueueWarps = 8;
+
+__global__ void __launch_bounds__(kSlabQueueWarps * 32)
+    msc_slab_queue_kernel(const MscHalf p, const SlabOffset so, long long total,
+                          long long per_warp, int nw_shift)
+{
+    __shared__ QueueSlots q_all[kSlabQueueWarps];
+    __shared__ uint4 lvmask[16];
+    if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+    __syncthreads();
+    const long long begin =
+        ((long long)blockIdx.x * kSlabQueueWarps + (threadIdx.x >> 5)) * per_warp;
+    const long long end = begin + per_warp < total ? begin + per_warp : total;
+    msc_queue_range<true>(p, begin, end, nw_shift, q_all[threadIdx.x >> 5], lvmask, so);
+}
+
+static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so, int sm_count,
+                                         int blocks_per_sm, cudaStream_t st)
+{
+    const long long total = (long long)p.rows * p.nw;
+    const long long warps = (long long)sm_count * blocks_per_sm * kSlabQueueWarps;
+    long long per_warp = (total + warps - 1) / warps;
+    per_warp = (per_warp + 31) / 32 * 32;
+    const long long nwarps = (total + per_warp - 1) / per_warp;
+    const unsigned blocks = (unsigned)((nwarps + kSlabQueueWarps - 1) / kSlabQueueWarps);
+    const int shift = (p.nw & (p.nw - 1)) == 0 ? __builtin_ctz((unsigned)p.nw) : -1;
+    msc_slab_queue_kernel<<<blocks, kSlabQueueWarps * 32, 0, st>>>(p, so, total, per_warp, shift);
+    return cudaGetLastError();
+}
+
 // The device seeded start of ising_fill_philox at global site indices.
 __global__ void slab_philox_int8_kernel(int8_t* c0, int8_t* c1, long long rows, long long row0,
                                         int lh, int pitch, u32 k0, u32 k1)
@@ -236,6 +269,13 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
         p.thr4 = s->table[3];
         p.thr8 = s->table[4];
         p.meas = meas;
+        p.nw_magic = magic_for(s->nw);
+        if (rule != kObserve && !meas) {
+            const cudaError_t e = launch_msc_slab_queue(
+                p, SlabOffset{s->row0 * s->nw, (int)(s->begin & 1)}, s->sm_count,
+                s->queue_blocks, s->stream);
+            return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
+        }
         const unsigned grid = slab_grid(s->rows * (long long)s->nw, s->max_blocks);
         if (rule == kObserve) msc_slab_kernel<false, true><<<grid, 256, 0, s->stream>>>(p, g);
         else if (meas) msc_slab_kernel<true, true><<<grid, 256, 0, s->stream>>>(p, g);
@@ -357,6 +397,14 @@ int ising_slab_create(int ndim, const int64_t* shape, int variant, int algorithm
     s->rule = select_rule(variant, algorithm, ndim, s->table);
     s->sm_count = device_sm_count(device);
     s->max_blocks = s->sm_count * 8;
+    {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_slab_queue_kernel,
+                                                          kSlabQueueWarps * 32, 0) == cudaSuccess &&
+            b > 0)
+            s->queue_blocks = b;
+        cudaGetLastError();
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete s;

@@ -275,3 +275,39 @@ def test_gpu_slab_argument_errors():
     with pytest.raises(ValueError):
         s.half_sweep(2, 0)
     s.close()
+
+
+def _nccl_world1_worker(port, queue):
+    import torch.distributed as dist
+
+    from pyising_b200.backend import B200Int8
+    from pyising_b200.slab import SlabSimulation
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        shape = (6, 8, 32)
+        one = B200Int8(shape, 0.25, seed=5, algorithm="heatbath", init="hot")
+        split = SlabSimulation(shape, 0.25, seed=5, algorithm="heatbath", init="hot",
+                               group="default")
+        ok = bool(np.array_equal(split.sweep_measured(6, 2), one.sweep_measured(6, 2)))
+        ok = ok and bool(np.array_equal(split.get_lattice(), one.get_lattice()))
+        ok = ok and split.observables_int() == one.observables_int()
+        split.close()
+        queue.put(ok)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_gpu_slab_process_group_world1_nccl():
+    """The process-group path (one slab per rank, NCCL all-reduce) on a world of one rank."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_world1_worker, args=(_free_port(), q))
+    p.start()
+    ok = q.get(timeout=240)
+    p.join(timeout=60)
+    assert p.exitcode == 0 and ok
