@@ -27,16 +27,31 @@ struct u32x4 {
 // One Philox4x32-10 block.  The counter words c1..c3 and the key are usually uniform across a
 // warp (sweep, colour, stream selector, seed), so the compiler keeps the first two rounds'
 // products in the uniform datapath; only the site/word index c0 varies per thread.
+// SPLIT: each 32x32->64 product as a separate high and low multiply (the same values); on
+// B200 that measured 4% faster inside the 2D int8 kernels, 1% slower in 3D and equal in msc.
+template <bool SPLIT = false>
 __device__ __forceinline__ u32x4 philox4x32_10(u32 c0, u32 c1, u32 c2, u32 c3, u32 k0, u32 k1)
 {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const u64 p0 = (u64)kPhiloxM0 * c0;
-        const u64 p1 = (u64)kPhiloxM1 * c2;
-        const u32 n0 = (u32)(p1 >> 32) ^ c1 ^ k0;
-        const u32 n2 = (u32)(p0 >> 32) ^ c3 ^ k1;
-        c1 = (u32)p1;
-        c3 = (u32)p0;
+        u32 h0, l0, h1, l1;
+        if constexpr (SPLIT) {
+            asm("mul.hi.u32 %0, %1, %2;" : "=r"(h0) : "r"(c0), "n"(kPhiloxM0));
+            asm("mul.lo.u32 %0, %1, %2;" : "=r"(l0) : "r"(c0), "n"(kPhiloxM0));
+            asm("mul.hi.u32 %0, %1, %2;" : "=r"(h1) : "r"(c2), "n"(kPhiloxM1));
+            asm("mul.lo.u32 %0, %1, %2;" : "=r"(l1) : "r"(c2), "n"(kPhiloxM1));
+        } else {
+            const u64 p0 = (u64)kPhiloxM0 * c0;
+            const u64 p1 = (u64)kPhiloxM1 * c2;
+            h0 = (u32)(p0 >> 32);
+            l0 = (u32)p0;
+            h1 = (u32)(p1 >> 32);
+            l1 = (u32)p1;
+        }
+        const u32 n0 = h1 ^ c1 ^ k0;
+        const u32 n2 = h0 ^ c3 ^ k1;
+        c1 = l1;
+        c3 = l0;
         c0 = n0;
         c2 = n2;
         k0 += kPhiloxW0;

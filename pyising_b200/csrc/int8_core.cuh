@@ -227,7 +227,8 @@ __device__ __forceinline__ Words<V / 4> int8_update(const Int8Half& p, long long
         if constexpr (RULE == kObserve) {
             ns.v[k] = s.v[k];
         } else {
-            const u32x4 r = philox4x32_10(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
+            const u32x4 r =
+                philox4x32_10<NDIM == 2>(q0 + (u32)k, p.t, p.color, 0u, p.k0, p.k1);
             const u32 d = decide4<NDIM, RULE>(p, s.v[k], cnt[k], r, stab);
             ns.v[k] = (!MIXED || k < wv) ? d : s.v[k];
         }
