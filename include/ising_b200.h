@@ -144,6 +144,10 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
 #define ISING_KNOB_BLOCKS_PER_SM 3
 #define ISING_KNOB_MSC_WAVES 4
 #define ISING_KNOB_GRAPH_CHUNK 5
+/* Cluster updates: sites per colour in a tile of the shared-memory union-find (0 = automatic,
+ * 1 = no tiles: one union-find in global memory, else 32..6144); the labels are the same for
+ * every value. */
+#define ISING_KNOB_CLUSTER_TILE 7
 /* Batch and server knobs (ising_batch_set_knob, ising_server_set_knob): ISING_KNOB_BAND is the
  * longest band a kernel class may use (default 8); ISING_KNOB_ITEMS_PER_SLOT the work items per
  * resident block a launch aims at (default 6; smaller items balance better, larger ones cost

@@ -526,6 +526,12 @@ int ising_set_knob(ising_sim* h, int knob, int value)
             return fail(ISING_ERR_INVALID, "graph chunk must be 1..%d sweeps", (int)kGraphChunkMax);
         h->graph_chunk = value;
         break;
+    case ISING_KNOB_CLUSTER_TILE:
+        if (value != 0 && value != 1 && (value < 32 || value > 6144))
+            return fail(ISING_ERR_INVALID,
+                        "cluster tile must be 0 (automatic), 1 (no tiles) or 32..6144");
+        h->cluster_tile = value;
+        break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
     clear_graphs(h);  // captured graphs hold the old launch parameters
@@ -542,6 +548,7 @@ int ising_get_knob(ising_sim* h, int knob, int* value)
     case ISING_KNOB_BLOCKS_PER_SM: *value = h->blocks_per_sm; break;
     case ISING_KNOB_MSC_WAVES: *value = h->msc_waves; break;
     case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
+    case ISING_KNOB_CLUSTER_TILE: *value = h->cluster_tile; break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
     return ISING_OK;

@@ -51,7 +51,8 @@ struct ising_sim {
     int schedule = ISING_SCHEDULE_AUTO;
     int mute_band = -1;                 // test hook of the persistent schedule
     unsigned int* d_flags = nullptr;    // persistent schedule: per-band progress + error word
-    int* d_label = nullptr;             // cluster updates: a label per site + error word
+    int* d_label = nullptr;             // cluster updates: a label per site, error word, masks
+    int cluster_tile = 0;               // cluster updates: positions per tile (0: automatic)
     bool pending_err = false;           // a persistent run's error word not yet read
 };
 

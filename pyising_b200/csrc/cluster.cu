@@ -7,15 +7,24 @@
 // connected components found by a lock-free union-find.
 //
 // One update at step t:
-//   1. every site is its own tree: label[g] = g;
-//   2. every bond joins a colour-0 site to a colour-1 site (the lattice is bipartite), so each
+//   1. every bond joins a colour-0 site to a colour-1 site (the lattice is bipartite), so each
 //      colour-0 site owns its 2d bonds and each bond is seen once.  A bond between aligned
 //      spins is active with probability p = 1 - exp(-2 beta) (threshold p_bond on a uniform
-//      u32 from Philox((n, t, kBondTag, k), key)); active bonds union their endpoints' trees:
-//      roots are linked larger-under-smaller with atomicCAS, finds halve paths with plain
-//      stores (parents only ever move up the tree, so a stale read is still an ancestor);
-//   3. every label is replaced by its root (a read-only walk: only thread i writes label[i]);
-//   4. every cluster flips with probability 1/2: bit (root & 127) of
+//      u32 from Philox((n, t, kBondTag, k), key)).  The union-find runs on two levels, so that
+//      the near-spanning clusters of the critical region do not funnel every union through a
+//      few global roots: a CTA owns a tile of T consecutive positions q of both colours
+//      (sites q and S + q) and unites the active bonds inside the tile in shared memory, then
+//      writes each site's tile-local root as its global label (sw_local_kernel); a second
+//      kernel unites the active bonds that leave their tile in global memory (sw_cross_kernel).
+//      Within a tile, pointer jumping then makes every node point at its root.  (The
+//      single-level variant, every bond united in global memory by sw_bond_kernel, is kept
+//      behind the cluster_tile knob.)
+//      On both levels roots are linked larger-under-smaller with atomicCAS and finds halve
+//      paths with plain stores (parents only ever move up the tree, so a stale read is still
+//      an ancestor); the tile order of sites is their global order, so the final root of a
+//      cluster is its smallest site whatever the tile size;
+//   2. every label is replaced by its root (a read-only walk: only thread i writes label[i]);
+//   3. every cluster flips with probability 1/2: bit (root & 127) of
 //      Philox((root >> 7, t, kFlipTag, 0), key), the same for all its sites.
 // Site g = c * S + row * lh + j (S = rows * lh sites per colour, the logical compressed index).
 // Labels are int32 (lattices of fewer than 2^31 sites).  Every retry loop is bounded: a thread
@@ -32,7 +41,7 @@ constexpr long long kUnionLimit = 1ll << 20;
 struct ClusterArgs {
     int8_t* c[2];
     int* label;
-    unsigned char* bonds;  // per colour-0 site, bit k = bond k active (diagnostics), or nullptr
+    unsigned char* bonds;  // per colour-0 site, bit k = bond k active
     int* err;
     long long S;           // sites per colour
     long long rows;
@@ -85,6 +94,134 @@ __device__ __forceinline__ void uf_union(int* label, int a, int b, int* err)
     atomicExch(err, 1);
 }
 
+// Colour-1 positions of the 2d bonds of colour-0 site n (the order of the bond bits): the same
+// index, the other horizontal neighbour, y + 1, y - 1, z + 1, z - 1 (periodic).
+__device__ __forceinline__ void bond_ends(const ClusterArgs& a, long long n, long long nb[6])
+{
+    const long long row = n / a.lh;
+    const int j = (int)(n - row * a.lh);
+    const int y = (int)(row % a.ly), z = (int)(row / a.ly);
+    const int par = (y + z) & 1;  // colour 0
+    const long long plane = (long long)z * a.ly;
+    nb[0] = row * a.lh + j;
+    nb[1] = row * a.lh + (par ? (j + 1 == a.lh ? 0 : j + 1) : (j == 0 ? a.lh - 1 : j - 1));
+    nb[2] = (plane + (y + 1 == a.ly ? 0 : y + 1)) * a.lh + j;
+    nb[3] = (plane + (y == 0 ? a.ly - 1 : y - 1)) * a.lh + j;
+    nb[4] = ((long long)(z + 1 == a.lz ? 0 : z + 1) * a.ly + y) * a.lh + j;
+    nb[5] = ((long long)(z == 0 ? a.lz - 1 : z - 1) * a.ly + y) * a.lh + j;
+}
+
+__device__ __forceinline__ int8_t colour1_spin(const ClusterArgs& a, long long m)
+{
+    const long long mrow = m / a.lh;
+    return a.c[1][mrow * a.pitch + (m - mrow * a.lh)];
+}
+
+// Shared-memory union-find of one tile (same rules as the global one).
+__device__ __forceinline__ int tile_find(volatile int* lab, int x, int* err)
+{
+    for (int it = 0; it < (1 << 20); ++it) {
+        const int p = lab[x];
+        if (p == x) return x;
+        const int gp = lab[p];
+        if (gp != p) lab[x] = gp;
+        x = gp;
+    }
+    atomicExch(err, 1);
+    return x;
+}
+
+__device__ __forceinline__ int tile_root(const volatile int* lab, int x, int* err)
+{
+    for (int it = 0; it < (1 << 20); ++it) {
+        const int p = lab[x];
+        if (p == x) return x;
+        x = p;
+    }
+    atomicExch(err, 1);
+    return x;
+}
+
+__device__ __forceinline__ void tile_union(int* lab, int a, int b, int* err)
+{
+    for (int it = 0; it < (1 << 20); ++it) {
+        a = tile_find(lab, a, err);
+        b = tile_find(lab, b, err);
+        if (a == b) return;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicCAS(lab + b, b, a);
+        if (old == b) return;
+        b = old;
+    }
+    atomicExch(err, 1);
+}
+
+// Tile b: positions [q0, q0 + n) of both colours, q0 = b * T; local index i (colour 0) and
+// T + i (colour 1) for position q0 + i.  Draws the bonds of the tile's colour-0 sites, stores
+// their masks, unites the active bonds that stay in the tile, and writes every tile site's
+// label: the global index of its tile-local root.
+__global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, int T)
+{
+    extern __shared__ int lab[];  // [2T]
+    const long long q0 = (long long)blockIdx.x * T;
+    const int n = (int)(a.S - q0 < T ? a.S - q0 : T);
+    for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) lab[i] = i;
+    __syncthreads();
+    const int nbonds = 2 * a.ndim;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const long long q = q0 + i;
+        const long long row = q / a.lh;
+        const int8_t s = a.c[0][row * a.pitch + (q - row * a.lh)];
+        long long nb[6];
+        bond_ends(a, q, nb);
+        const u32x4 r0 = philox4x32_10((u32)q, a.t, kBondTag, 0u, a.k0, a.k1);
+        u32x4 r1 = {0u, 0u, 0u, 0u};
+        if (a.ndim == 3) r1 = philox4x32_10((u32)q, a.t, kBondTag, 1u, a.k0, a.k1);
+        const u32 u[6] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y};
+        unsigned mask = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            if (k >= nbonds) break;
+            if (u[k] < a.p_bond && colour1_spin(a, nb[k]) == s) {
+                mask |= 1u << k;
+                const long long d = nb[k] - q0;
+                if (d >= 0 && d < n) tile_union(lab, i, T + (int)d, a.err);
+            }
+        }
+        a.bonds[q] = (unsigned char)mask;
+    }
+    __syncthreads();
+    // Pointer jumping until every node points at its root: a concurrent reader sees the old
+    // parent or the grandparent, both ancestors, so walks stay valid; log2(depth) rounds.
+    volatile int* vlab = lab;
+    for (int round = 0; round < 32; ++round) {
+        int changed = 0;
+        for (int i = threadIdx.x; i < 2 * n; i += blockDim.x) {
+            const int li = i < n ? i : T + (i - n);
+            const int p = vlab[li];
+            const int gp = vlab[p];
+            if (gp != p) {
+                vlab[li] = gp;
+                changed = 1;
+            }
+        }
+        if (!__syncthreads_or(changed)) break;
+    }
+    for (int i = threadIdx.x; i < 2 * n; i += blockDim.x) {
+        const int li = i < n ? i : T + (i - n);
+        const int r = tile_root(lab, li, a.err);
+        const long long gi = li < T ? q0 + li : a.S + q0 + (li - T);
+        const long long gr = r < T ? q0 + r : a.S + q0 + (r - T);
+        a.label[gi] = (int)gr;
+    }
+}
+
+// Single-level variant (cluster_tile knob 1): every site its own tree, then every colour-0 site
+// draws its bonds and unites the active ones in global memory directly.
 __global__ void sw_init_kernel(int* label, long long n)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -94,41 +231,48 @@ __global__ void sw_init_kernel(int* label, long long n)
 
 __global__ void sw_bond_kernel(const ClusterArgs a)
 {
-    const long long n0 = a.S;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < n0;
-         n += (long long)gridDim.x * blockDim.x) {
-        const long long row = n / a.lh;
-        const int j = (int)(n - row * a.lh);
-        const int y = (int)(row % a.ly), z = (int)(row / a.ly);
-        const int par = (y + z) & 1;  // colour 0
-        const int8_t s = a.c[0][row * a.pitch + j];
-        // the 2d colour-1 neighbours: same index, the other horizontal one, y -+ 1, z -+ 1
+    const int nbonds = 2 * a.ndim;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.S;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long row = q / a.lh;
+        const int8_t s = a.c[0][row * a.pitch + (q - row * a.lh)];
         long long nb[6];
-        const long long plane = (long long)z * a.ly;
-        nb[0] = row * a.lh + j;
-        nb[1] = row * a.lh + (par ? (j + 1 == a.lh ? 0 : j + 1) : (j == 0 ? a.lh - 1 : j - 1));
-        nb[2] = (plane + (y + 1 == a.ly ? 0 : y + 1)) * a.lh + j;
-        nb[3] = (plane + (y == 0 ? a.ly - 1 : y - 1)) * a.lh + j;
-        nb[4] = ((long long)(z + 1 == a.lz ? 0 : z + 1) * a.ly + y) * a.lh + j;
-        nb[5] = ((long long)(z == 0 ? a.lz - 1 : z - 1) * a.ly + y) * a.lh + j;
-        const u32x4 r0 = philox4x32_10((u32)n, a.t, kBondTag, 0u, a.k0, a.k1);
+        bond_ends(a, q, nb);
+        const u32x4 r0 = philox4x32_10((u32)q, a.t, kBondTag, 0u, a.k0, a.k1);
         u32x4 r1 = {0u, 0u, 0u, 0u};
-        if (a.ndim == 3) r1 = philox4x32_10((u32)n, a.t, kBondTag, 1u, a.k0, a.k1);
+        if (a.ndim == 3) r1 = philox4x32_10((u32)q, a.t, kBondTag, 1u, a.k0, a.k1);
         const u32 u[6] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y};
         unsigned mask = 0;
-        const int nbonds = 2 * a.ndim;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             if (k >= nbonds) break;
-            const long long m = nb[k];
-            const long long mrow = m / a.lh;
-            const int8_t sn = a.c[1][mrow * a.pitch + (m - mrow * a.lh)];
-            if (sn == s && u[k] < a.p_bond) {
+            if (u[k] < a.p_bond && colour1_spin(a, nb[k]) == s) {
                 mask |= 1u << k;
-                uf_union(a.label, (int)n, (int)(n0 + m), a.err);
+                uf_union(a.label, (int)q, (int)(a.S + nb[k]), a.err);
             }
         }
-        if (a.bonds) a.bonds[n] = (unsigned char)mask;
+        a.bonds[q] = (unsigned char)mask;
+    }
+}
+
+// The active bonds that leave their colour-0 site's tile, united in global memory.
+__global__ void sw_cross_kernel(const ClusterArgs a, int T)
+{
+    const int nbonds = 2 * a.ndim;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.S;
+         q += (long long)gridDim.x * blockDim.x) {
+        const unsigned mask = a.bonds[q];
+        if (!mask) continue;
+        const long long q0 = q / T * T;
+        const long long q1 = q0 + T < a.S ? q0 + T : a.S;
+        long long nb[6];
+        bond_ends(a, q, nb);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            if (k >= nbonds) break;
+            if (((mask >> k) & 1u) && (nb[k] < q0 || nb[k] >= q1))
+                uf_union(a.label, (int)q, (int)(a.S + nb[k]), a.err);
+        }
     }
 }
 
@@ -153,7 +297,7 @@ __global__ void sw_flip_kernel(const ClusterArgs a)
             const int c = g >= a.S ? 1 : 0;
             const long long m = g - (long long)c * a.S;
             const long long row = m / a.lh;
-            int8_t* p = a.c[c] + row * a.pitch + (m - row * a.lh);
+            int8_t* p = (c ? a.c[1] : a.c[0]) + row * a.pitch + (m - row * a.lh);
             *p = (int8_t)(*p ^ (int8_t)0xFE);  // +1 <-> -1
         }
     }
@@ -166,8 +310,9 @@ static int cluster_setup(ising_sim* h)
     const long long n = 2 * h->rows * (long long)h->lh;
     if (n >= 0x7FFFFFFFll)
         return fail(ISING_ERR_INVALID, "cluster updates: lattices of fewer than 2^31 sites");
-    if (!h->d_label) {
-        cudaError_t e = cudaMalloc((void**)&h->d_label, (size_t)n * sizeof(int) + 256);
+    if (!h->d_label) {  // labels, the error word, then one bond mask per colour-0 site
+        cudaError_t e =
+            cudaMalloc((void**)&h->d_label, (size_t)n * sizeof(int) + 256 + (size_t)(n / 2));
         if (e != cudaSuccess) {
             cudaGetLastError();
             return fail(ISING_ERR_NOMEM, "cudaMalloc of the cluster labels (%lld sites)", n);
@@ -176,9 +321,26 @@ static int cluster_setup(ising_sim* h)
     return ISING_OK;
 }
 
-// One labeling (steps 1-3) and, when `flip`, the cluster flips (step 4).
-static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip,
-                        unsigned char* bonds)
+// Positions per tile of the shared-memory union-find (2 ints each): the handle's cluster_tile
+// knob (1 = no tiles: the single-level union-find in global memory), else kTileAuto.  Small
+// tiles give many CTAs and short trees; measured per update on B200 (single-level / 256-position
+// tiles): 256^2 53 / 39 us, 1024^2 200 / 113 us, 4096^2 2964 / 1212 us, 256^3 2988 / 1258 us.
+constexpr int kTileAuto = 256;
+
+static int cluster_tile_size(const ising_sim* h, long long S)
+{
+    if (h->cluster_tile == 1) return 0;
+    const long long T = h->cluster_tile > 0 ? h->cluster_tile : kTileAuto;
+    return (int)(T > S ? S : T);
+}
+
+static unsigned char* cluster_masks(ising_sim* h, long long S)
+{
+    return reinterpret_cast<unsigned char*>(h->d_label) + 2 * S * sizeof(int) + 256;
+}
+
+// One labeling (step 1-2) and, when `flip`, the cluster flips (step 3).
+static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip)
 {
     ClusterArgs a;
     a.c[0] = (int8_t*)h->c[0];
@@ -186,7 +348,7 @@ static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip,
     a.S = h->rows * (long long)h->lh;
     a.label = h->d_label;
     a.err = reinterpret_cast<int*>(reinterpret_cast<char*>(h->d_label) + 2 * a.S * sizeof(int));
-    a.bonds = bonds;
+    a.bonds = cluster_masks(h, a.S);
     a.rows = h->rows;
     a.lh = h->lh;
     a.ly = h->ly;
@@ -198,8 +360,15 @@ static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip,
     a.k1 = (u32)(seed >> 32);
     a.p_bond = p_bond;
     const int grid = h->sm_count * 8;
-    sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
-    sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);
+    const int T = cluster_tile_size(h, a.S);
+    if (T > 0) {
+        const unsigned tiles = (unsigned)((a.S + T - 1) / T);
+        sw_local_kernel<<<tiles, 256, (size_t)2 * T * sizeof(int), h->stream>>>(a, T);
+        sw_cross_kernel<<<grid, 256, 0, h->stream>>>(a, T);
+    } else {
+        sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
+        sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);
+    }
     sw_flatten_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S, a.err);
     if (flip) sw_flip_kernel<<<grid, 256, 0, h->stream>>>(a);
     const cudaError_t e = cudaGetLastError();
@@ -243,7 +412,7 @@ extern "C" int ising_cluster_sweep(ising_sim* h, uint64_t step0, int64_t n_steps
                         h->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     for (int64_t k = 0; k < n_steps; ++k) {
-        rc = cluster_step(h, (u32)(step0 + (uint64_t)k), seed, p_bond, true, nullptr);
+        rc = cluster_step(h, (u32)(step0 + (uint64_t)k), seed, p_bond, true);
         if (rc == ISING_OK && series_out)
             rc = observe(h, reinterpret_cast<unsigned long long*>(h->d_series + 2 * k));
         if (rc != ISING_OK) return rc;
@@ -267,26 +436,19 @@ extern "C" int ising_cluster_labels(ising_sim* h, uint64_t step, uint64_t seed, 
     int rc = cluster_setup(h);
     if (rc != ISING_OK) return rc;
     const long long S = h->rows * (long long)h->lh;
-    unsigned char* d_bonds = nullptr;
-    e = cudaMalloc((void**)&d_bonds, (size_t)S);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (bonds)");
     e = cudaMemsetAsync(reinterpret_cast<char*>(h->d_label) + 2 * S * sizeof(int), 0, sizeof(int),
                         h->stream);
-    if (e == cudaSuccess) {
-        rc = cluster_step(h, (u32)step, seed, p_bond, false, d_bonds);
-        if (rc == ISING_OK) rc = cluster_error(h);
-        if (rc == ISING_OK) {
-            e = cudaMemcpyAsync(labels_out, h->d_label, (size_t)(2 * S) * sizeof(int),
-                                cudaMemcpyDeviceToHost, h->stream);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(bonds_out, d_bonds, (size_t)S, cudaMemcpyDeviceToHost,
-                                    h->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-            if (e != cudaSuccess) rc = cuda_fail(e, "cluster labels copy");
-        }
-    } else {
-        rc = cuda_fail(e, "cudaMemsetAsync");
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    rc = cluster_step(h, (u32)step, seed, p_bond, false);
+    if (rc == ISING_OK) rc = cluster_error(h);
+    if (rc == ISING_OK) {
+        e = cudaMemcpyAsync(labels_out, h->d_label, (size_t)(2 * S) * sizeof(int),
+                            cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(bonds_out, cluster_masks(h, S), (size_t)S, cudaMemcpyDeviceToHost,
+                                h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cluster labels copy");
     }
-    cudaFree(d_bonds);
     return rc;
 }

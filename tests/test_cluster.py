@@ -50,12 +50,26 @@ def components_min(n, edges):
     return np.array([find(x) for x in range(n)])
 
 
+KNOB_CLUSTER_TILE = 7
+
+
+def set_cluster_tile(sim, tile):
+    from pyising_b200._lib import check, lib
+
+    check(lib().ising_set_knob(sim._h, KNOB_CLUSTER_TILE, int(tile)), "set_knob")
+
+
+# tile 0: automatic (256 positions: one tile for the 2D cases, two for 3D); 1: single-level;
+# 32 and 100: many tiles, rows split across tiles, so most bonds are united by the cross-tile
+# kernel; 6144: one tile holding the whole lattice
+@pytest.mark.parametrize("tile", [0, 1, 32, 100, 6144])
 @pytest.mark.parametrize("shape,beta", [((16, 32), 0.3), ((16, 32), 0.7), ((24, 40), 0.44),
                                         ((8, 8, 16), 0.22), ((8, 8, 16), 0.5)])
-def test_labels_are_the_components_of_the_active_bonds(oracle_mod, shape, beta):
+def test_labels_are_the_components_of_the_active_bonds(oracle_mod, shape, beta, tile):
     from pyising_b200.backend import B200Int8
 
     sim = B200Int8(shape, beta, seed=77, init=oracle_mod.random_lattice(shape, 5))
+    set_cluster_tile(sim, tile)
     sim.sweep(3)
     c0, c1 = sim.colour_arrays()
     labels, bonds = sim.cluster_labels(step=9)
@@ -77,6 +91,31 @@ def test_labels_are_the_components_of_the_active_bonds(oracle_mod, shape, beta):
     np.testing.assert_array_equal(labels.reshape(-1), want)
     p = 1.0 - math.exp(-2.0 * beta)
     assert abs(active - p * aligned) < 5 * math.sqrt(aligned * p * (1 - p)) + 1
+
+
+def test_cluster_updates_do_not_depend_on_the_tile_size():
+    from pyising_b200.backend import B200Int8
+
+    out = []
+    for shape, tile in [((128, 96), 0), ((128, 96), 32), ((128, 96), 1000), ((128, 96), 6144),
+                        ((16, 24, 32), 0), ((16, 24, 32), 77), ((16, 24, 32), 1024)]:
+        sim = B200Int8(shape, 0.44 if len(shape) == 2 else 0.22, seed=9, init="hot")
+        set_cluster_tile(sim, tile)
+        series = sim.cluster_sweep(6, measure=True)
+        out.append((shape, series, sim.get_lattice()))
+    for (shape_a, sa, la), (shape_b, sb, lb) in zip(out, out[1:]):
+        if shape_a == shape_b:
+            np.testing.assert_array_equal(sa, sb)
+            np.testing.assert_array_equal(la, lb)
+
+
+def test_cluster_tile_knob_range():
+    from pyising_b200.backend import B200Int8
+
+    sim = B200Int8((16, 16), 0.4, init="cold")
+    for bad in (-1, 2, 31, 6145):
+        with pytest.raises(ValueError):
+            set_cluster_tile(sim, bad)
 
 
 def test_cluster_sweeps_are_deterministic_and_keep_the_lattice_valid():
