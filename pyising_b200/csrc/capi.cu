@@ -123,11 +123,12 @@ static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* 
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
     int rc = ISING_OK;
     const bool tb = use_temporal(h);
+    const int K = temporal_sweeps();
     for (int64_t s = 0; s < G && rc == ISING_OK;) {
-        if (tb && s + 2 <= G - (measured ? 1 : 0)) {  // two unmeasured sweeps in one launch
+        if (tb && s + K <= G - (measured ? 1 : 0)) {  // K unmeasured sweeps in one launch
             const cudaError_t le = launch_int8_temporal(h, (u32)s, ctl);
             if (le != cudaSuccess) rc = cuda_fail(le, "temporal half-sweeps");
-            s += 2;
+            s += K;
             continue;
         }
         unsigned long long* m =
@@ -662,13 +663,20 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
         }
     }
     const bool tb = use_temporal(h);
+    const int K = temporal_sweeps();
+    // sweeps s .. s + K - 1 hold no measurement
+    auto unmeasured = [&](int64_t s) {
+        if (measure_every <= 0) return true;
+        for (int i = 0; i < K; ++i)
+            if ((s + i + 1) % measure_every == 0) return false;
+        return true;
+    };
     for (int64_t s = s0; s < n_sweeps; ++s) {
         const u32 t = (u32)(t0 + (uint64_t)s);
         const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;
-        if (tb && !meas && s + 2 <= n_sweeps &&
-            !(measure_every > 0 && (s + 2) % measure_every == 0)) {
-            TRY_CUDA(launch_int8_temporal(h, t, nullptr));  // sweeps s and s + 1
-            ++s;
+        if (tb && s + K <= n_sweeps && unmeasured(s)) {
+            TRY_CUDA(launch_int8_temporal(h, t, nullptr));  // sweeps s .. s + K - 1
+            s += K - 1;
             continue;
         }
         unsigned long long* m = meas ? (unsigned long long*)(h->d_series + 2 * k) : nullptr;

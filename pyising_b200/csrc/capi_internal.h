@@ -71,6 +71,7 @@ void clear_graphs(ising_sim* h);
 int observe(ising_sim* h, unsigned long long* acc);
 bool temporal_ok(const ising_sim* h);
 cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long long* ctl);
+int temporal_sweeps();  // sweeps per temporal launch
 int run_persistent_int8(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
                         unsigned long long* series, unsigned int* flags, int* err, int mute_band);
 int selftest_bounded_wait(int device, int* timed_out);

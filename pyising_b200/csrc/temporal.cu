@@ -23,7 +23,11 @@ namespace ising {
 #define ISING_TB_BAND 8
 #endif
 constexpr int kTbBand = ISING_TB_BAND;           // rows a CTA writes back
-constexpr int kTbSteps = 4;                      // half-sweeps per launch: two sweeps
+#ifndef ISING_TB_STEPS
+#define ISING_TB_STEPS 4
+#endif
+constexpr int kTbSteps = ISING_TB_STEPS;         // half-sweeps per launch (even: whole sweeps)
+static_assert(kTbSteps % 2 == 0, "whole sweeps per launch");
 constexpr int kTbRows = kTbBand + 2 * kTbSteps;  // tile rows per colour
 constexpr int kTbMaxSmem = 96 * 1024;
 #ifndef ISING_TB_THREADS
@@ -140,7 +144,9 @@ bool temporal_ok(const ising_sim* h)
            2 * kTbRows * h->lh <= kTbMaxSmem;
 }
 
-// Two sweeps from sweep t (relative to ctl[0] when ctl is set), colour 0 first.
+int temporal_sweeps() { return kTbSteps / 2; }
+
+// kTbSteps / 2 sweeps from sweep t (relative to ctl[0] when ctl is set), colour 0 first.
 cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long long* ctl)
 {
     Int8Half p;
