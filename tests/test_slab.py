@@ -39,6 +39,53 @@ def test_partition_covers_the_axis():
         partition(4, 0)
 
 
+@pytest.mark.parametrize("ndim,shape,variant,begin,count,msg", [
+    (2, (16, 16, 0), 0, 0, 0, "outside the first axis"),
+    (2, (16, 16, 0), 0, 10, 8, "outside the first axis"),
+    (2, (16, 16, 0), 0, -1, 4, "outside the first axis"),
+    (3, (8, 8, 128), 1, 0, 4, "2D Metropolis"),
+    (2, (16, 12, 0), 0, 0, 4, "multiple of 8"),
+    (4, (8, 8, 8), 0, 0, 4, "2D and 3D"),
+])
+def test_slab_create_validates_before_touching_cuda(ndim, shape, variant, begin, count, msg):
+    import ctypes
+
+    from pyising_b200._lib import lib
+
+    h = ctypes.c_void_p()
+    arr = (ctypes.c_int64 * 3)(*shape)
+    rc = lib().ising_slab_create(ndim, arr, variant, 0, 0, begin, count, 0, ctypes.byref(h))
+    assert rc == 1  # ISING_ERR_INVALID
+    assert msg in lib().ising_last_error().decode()
+    assert not h.value
+
+
+def test_slab_calls_reject_null_handles():
+    from pyising_b200._lib import lib
+
+    L = lib()
+    assert L.ising_slab_destroy(None) == 0
+    assert L.ising_slab_half_sweep(None, 0, 0, -1) == 1
+    assert "null" in L.ising_last_error().decode()
+    assert L.ising_slab_halo(None, 0, 0, None, None) == 1
+    assert L.ising_slab_observables(None, None, None) == 1
+
+
+@pytest.mark.parametrize("shape", [(6, 16), (4, 6, 8), (10, 256)])
+def test_host_colour_split_matches_the_oracle(shape):
+    from pyising_b200.lattice import merge_colours, pack_colour, split_colours, unpack_colour
+
+    lat = oracle.random_lattice(shape, 4)
+    c0, c1 = split_colours(lat)
+    w0, w1 = oracle.to_compressed(lat)
+    np.testing.assert_array_equal(c0, w0)
+    np.testing.assert_array_equal(c1, w1)
+    np.testing.assert_array_equal(merge_colours(c0, c1, shape), lat)
+    if shape[-1] % 128 == 0:
+        np.testing.assert_array_equal(pack_colour(c0), oracle.pack_bits(w0))
+        np.testing.assert_array_equal(unpack_colour(pack_colour(c1)), c1)
+
+
 class CpuSlab:
     """A slab of an int8 lattice on the CPU with the C-ABI slab's interface: rows
     [begin, begin + count) of the first axis plus one halo row (2D) or plane (3D) per side,
