@@ -12,8 +12,8 @@
 //      spins is active with probability p = 1 - exp(-2 beta) (threshold p_bond on a uniform
 //      u32 from Philox((n, t, kBondTag, k), key)).  The union-find runs on two levels, so that
 //      the near-spanning clusters of the critical region do not funnel every union through a
-//      few global roots: a CTA owns a tile of T consecutive positions q of both colours
-//      (sites q and S + q) and unites the active bonds inside the tile in shared memory, then
+//      few global roots: a CTA owns a tile of R rows x W positions of one plane, both colours
+//      (16 x 32 by default), unites the active bonds inside the tile in shared memory, then
 //      writes each site's tile-local root as its global label (sw_local_kernel); a second
 //      kernel unites the active bonds that leave their tile in global memory (sw_cross_kernel).
 //      Within a tile, pointer jumping then makes every node point at its root.  (The
@@ -160,24 +160,69 @@ __device__ __forceinline__ void tile_union(int* lab, int a, int b, int* err)
     atomicExch(err, 1);
 }
 
-// Tile b: positions [q0, q0 + n) of both colours, q0 = b * T; local index i (colour 0) and
-// T + i (colour 1) for position q0 + i.  Draws the bonds of the tile's colour-0 sites, stores
-// their masks, unites the active bonds that stay in the tile, and writes every tile site's
-// label: the global index of its tile-local root.
-__global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, int T)
+// Rectangular tiles: a tile is R rows x W positions of one plane (y in [y0, y0 + R), j in
+// [j0, j0 + W), clipped at the plane's edges), of both colours; its local index of position
+// (r, c) is r * W + c for colour 0 and R * W + r * W + c for colour 1, which orders a tile's
+// sites as their global indices do.
+struct TileGeo {
+    int R, W;        // rows and positions per tile
+    int tx, ty;      // tiles per row of positions, per plane
+};
+
+__device__ __forceinline__ void tile_origin(const ClusterArgs& a, const TileGeo& g, long long b,
+                                           int& z, int& y0, int& j0)
 {
-    extern __shared__ int lab[];  // [2T]
-    const long long q0 = (long long)blockIdx.x * T;
-    const int n = (int)(a.S - q0 < T ? a.S - q0 : T);
-    for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) lab[i] = i;
+    const long long per_plane = (long long)g.tx * g.ty;
+    z = (int)(b / per_plane);
+    const int rem = (int)(b - (long long)z * per_plane);
+    const int by = rem / g.tx;
+    y0 = by * g.R;
+    j0 = (rem - by * g.tx) * g.W;
+}
+
+// Colour-1 coordinates (y, j, z) of bond k of colour-0 site (y, j, z) (the order of the bond
+// bits), periodic.
+__device__ __forceinline__ void bond_end(const ClusterArgs& a, int k, int y, int j, int z,
+                                         int& ny, int& nj, int& nz)
+{
+    ny = y;
+    nj = j;
+    nz = z;
+    if (k == 1) {
+        const int par = (y + z) & 1;  // colour 0
+        nj = par ? (j + 1 == a.lh ? 0 : j + 1) : (j == 0 ? a.lh - 1 : j - 1);
+    } else if (k == 2) {
+        ny = y + 1 == a.ly ? 0 : y + 1;
+    } else if (k == 3) {
+        ny = y == 0 ? a.ly - 1 : y - 1;
+    } else if (k == 4) {
+        nz = z + 1 == a.lz ? 0 : z + 1;
+    } else if (k == 5) {
+        nz = z == 0 ? a.lz - 1 : z - 1;
+    }
+}
+
+// Tile b: draws the bonds of the tile's colour-0 sites, stores their masks, unites the active
+// bonds that stay in the tile (shared memory), flattens the tile's trees and writes every tile
+// site's label: the global index of its tile-local root.
+__global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, const TileGeo g)
+{
+    extern __shared__ int lab[];  // [2 R W]
+    int z, y0, j0;
+    tile_origin(a, g, blockIdx.x, z, y0, j0);
+    const int R = g.R, W = g.W, RW = R * W;
+    const int rn = a.ly - y0 < R ? a.ly - y0 : R;  // rows of this tile
+    const int wn = a.lh - j0 < W ? a.lh - j0 : W;  // positions per row of this tile
+    for (int i = threadIdx.x; i < 2 * RW; i += blockDim.x) lab[i] = i;
     __syncthreads();
     const int nbonds = 2 * a.ndim;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const long long q = q0 + i;
-        const long long row = q / a.lh;
-        const int8_t s = a.c[0][row * a.pitch + (q - row * a.lh)];
-        long long nb[6];
-        bond_ends(a, q, nb);
+    const long long plane = (long long)z * a.ly;
+    for (int i = threadIdx.x; i < rn * wn; i += blockDim.x) {
+        const int r = i / wn, c = i - (i / wn) * wn;
+        const int y = y0 + r, j = j0 + c;
+        const long long row = plane + y;
+        const long long q = row * a.lh + j;
+        const int8_t s = a.c[0][row * a.pitch + j];
         const u32x4 r0 = philox4x32_10((u32)q, a.t, kBondTag, 0u, a.k0, a.k1);
         u32x4 r1 = {0u, 0u, 0u, 0u};
         if (a.ndim == 3) r1 = philox4x32_10((u32)q, a.t, kBondTag, 1u, a.k0, a.k1);
@@ -186,11 +231,14 @@ __global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, int 
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             if (k >= nbonds) break;
-            if (u[k] < a.p_bond && colour1_spin(a, nb[k]) == s) {
-                mask |= 1u << k;
-                const long long d = nb[k] - q0;
-                if (d >= 0 && d < n) tile_union(lab, i, T + (int)d, a.err);
-            }
+            if (u[k] >= a.p_bond) continue;
+            int ny, nj, nz;
+            bond_end(a, k, y, j, z, ny, nj, nz);
+            const long long nrow = (long long)nz * a.ly + ny;
+            if (a.c[1][nrow * a.pitch + nj] != s) continue;
+            mask |= 1u << k;
+            if (nz == z && ny >= y0 && ny < y0 + rn && nj >= j0 && nj < j0 + wn)
+                tile_union(lab, r * W + c, RW + (ny - y0) * W + (nj - j0), a.err);
         }
         a.bonds[q] = (unsigned char)mask;
     }
@@ -200,8 +248,10 @@ __global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, int 
     volatile int* vlab = lab;
     for (int round = 0; round < 32; ++round) {
         int changed = 0;
-        for (int i = threadIdx.x; i < 2 * n; i += blockDim.x) {
-            const int li = i < n ? i : T + (i - n);
+        for (int i = threadIdx.x; i < 2 * rn * wn; i += blockDim.x) {
+            const int cc = i >= rn * wn;
+            const int ii = i - cc * rn * wn;
+            const int li = cc * RW + (ii / wn) * W + (ii - (ii / wn) * wn);
             const int p = vlab[li];
             const int gp = vlab[p];
             if (gp != p) {
@@ -211,11 +261,16 @@ __global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, int 
         }
         if (!__syncthreads_or(changed)) break;
     }
-    for (int i = threadIdx.x; i < 2 * n; i += blockDim.x) {
-        const int li = i < n ? i : T + (i - n);
-        const int r = tile_root(lab, li, a.err);
-        const long long gi = li < T ? q0 + li : a.S + q0 + (li - T);
-        const long long gr = r < T ? q0 + r : a.S + q0 + (r - T);
+    for (int i = threadIdx.x; i < 2 * rn * wn; i += blockDim.x) {
+        const int cc = i >= rn * wn;
+        const int ii = i - cc * rn * wn;
+        const int r = ii / wn, c = ii - (ii / wn) * wn;
+        const int li = cc * RW + r * W + c;
+        const int root = tile_root(lab, li, a.err);
+        const int rc = root >= RW;
+        const int rl = root - rc * RW;
+        const long long gi = (long long)cc * a.S + (plane + y0 + r) * a.lh + j0 + c;
+        const long long gr = (long long)rc * a.S + (plane + y0 + rl / W) * a.lh + j0 + rl % W;
         a.label[gi] = (int)gr;
     }
 }
@@ -256,22 +311,26 @@ __global__ void sw_bond_kernel(const ClusterArgs a)
 }
 
 // The active bonds that leave their colour-0 site's tile, united in global memory.
-__global__ void sw_cross_kernel(const ClusterArgs a, int T)
+__global__ void sw_cross_kernel(const ClusterArgs a, const TileGeo g)
 {
     const int nbonds = 2 * a.ndim;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.S;
          q += (long long)gridDim.x * blockDim.x) {
         const unsigned mask = a.bonds[q];
         if (!mask) continue;
-        const long long q0 = q / T * T;
-        const long long q1 = q0 + T < a.S ? q0 + T : a.S;
-        long long nb[6];
-        bond_ends(a, q, nb);
+        const long long row = q / a.lh;
+        const int j = (int)(q - row * a.lh);
+        const int y = (int)(row % a.ly), z = (int)(row / a.ly);
+        const int y0 = y / g.R * g.R, j0 = j / g.W * g.W;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             if (k >= nbonds) break;
-            if (((mask >> k) & 1u) && (nb[k] < q0 || nb[k] >= q1))
-                uf_union(a.label, (int)q, (int)(a.S + nb[k]), a.err);
+            if (!((mask >> k) & 1u)) continue;
+            int ny, nj, nz;
+            bond_end(a, k, y, j, z, ny, nj, nz);
+            if (nz == z && ny >= y0 && ny < y0 + g.R && nj >= j0 && nj < j0 + g.W) continue;
+            const long long m = ((long long)nz * a.ly + ny) * a.lh + nj;
+            uf_union(a.label, (int)q, (int)(a.S + m), a.err);
         }
     }
 }
@@ -321,17 +380,26 @@ static int cluster_setup(ising_sim* h)
     return ISING_OK;
 }
 
-// Positions per tile of the shared-memory union-find (2 ints each): the handle's cluster_tile
-// knob (1 = no tiles: the single-level union-find in global memory), else kTileAuto.  Small
-// tiles give many CTAs and short trees; measured per update on B200 (single-level / 256-position
-// tiles): 256^2 53 / 39 us, 1024^2 200 / 113 us, 4096^2 2964 / 1212 us, 256^3 2988 / 1258 us.
-constexpr int kTileAuto = 256;
+// Tile shape of the shared-memory union-find: about T positions (the handle's cluster_tile
+// knob, else kTileAuto) as R rows x W positions, W = 32 (16 for small T) or the row length;
+// T = 0: the single-level union-find in global memory (knob value 1).  Small tiles give many
+// CTAs and short trees, square-ish ones keep most bonds inside their tile.  Measured per update
+// on B200 (single-level / 16 x 32 tiles): 256^2 52 / 39 us, 1024^2 199 / 85 us, 4096^2 2969 /
+// 813 us, 256^3 2996 / 1062 us.
+constexpr int kTileAuto = 512;
 
-static int cluster_tile_size(const ising_sim* h, long long S)
+static int cluster_tiles(const ising_sim* h, TileGeo* g)
 {
     if (h->cluster_tile == 1) return 0;
-    const long long T = h->cluster_tile > 0 ? h->cluster_tile : kTileAuto;
-    return (int)(T > S ? S : T);
+    const int T = h->cluster_tile > 0 ? h->cluster_tile : kTileAuto;
+    g->W = T >= 256 ? 32 : 16;
+    if (g->W > h->lh) g->W = h->lh;
+    g->R = T / g->W;
+    if (g->R < 1) g->R = 1;
+    if (g->R > h->ly) g->R = h->ly;
+    g->tx = (h->lh + g->W - 1) / g->W;
+    g->ty = (h->ly + g->R - 1) / g->R;
+    return g->tx * g->ty * h->lz;
 }
 
 static unsigned char* cluster_masks(ising_sim* h, long long S)
@@ -360,11 +428,12 @@ static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip)
     a.k1 = (u32)(seed >> 32);
     a.p_bond = p_bond;
     const int grid = h->sm_count * 8;
-    const int T = cluster_tile_size(h, a.S);
-    if (T > 0) {
-        const unsigned tiles = (unsigned)((a.S + T - 1) / T);
-        sw_local_kernel<<<tiles, 256, (size_t)2 * T * sizeof(int), h->stream>>>(a, T);
-        sw_cross_kernel<<<grid, 256, 0, h->stream>>>(a, T);
+    TileGeo g;
+    const int tiles = cluster_tiles(h, &g);
+    if (tiles > 0) {
+        sw_local_kernel<<<(unsigned)tiles, 256, (size_t)2 * g.R * g.W * sizeof(int), h->stream>>>(
+            a, g);
+        sw_cross_kernel<<<grid, 256, 0, h->stream>>>(a, g);
     } else {
         sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
         sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);

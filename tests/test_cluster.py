@@ -59,9 +59,9 @@ def set_cluster_tile(sim, tile):
     check(lib().ising_set_knob(sim._h, KNOB_CLUSTER_TILE, int(tile)), "set_knob")
 
 
-# tile 0: automatic (256 positions: one tile for the 2D cases, two for 3D); 1: single-level;
-# 32 and 100: many tiles, rows split across tiles, so most bonds are united by the cross-tile
-# kernel; 6144: one tile holding the whole lattice
+# tile 0: automatic (16 rows x 32 positions); 1: single-level; 32 and 100: tiles of 2 and 6 rows
+# x 16 positions, so many bonds are united by the cross-tile kernel; 6144: tiles as tall as the
+# lattice
 @pytest.mark.parametrize("tile", [0, 1, 32, 100, 6144])
 @pytest.mark.parametrize("shape,beta", [((16, 32), 0.3), ((16, 32), 0.7), ((24, 40), 0.44),
                                         ((8, 8, 16), 0.22), ((8, 8, 16), 0.5)])
