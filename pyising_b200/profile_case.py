@@ -1,13 +1,15 @@
 """Run one small sweep case, for profilers (ncu) and quick timing.
 
-    python -m pyising_b200.profile_case {int8|hb3|msc|sw|batch} L SWEEPS
+    python -m pyising_b200.profile_case {int8|hb3|msc|sw|batch|batch1} L SWEEPS
 
 int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
 beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7;
 sw: SWEEPS Swendsen-Wang updates of a 2D int8 L x L lattice at beta_c from a cold start;
 batch: an ensemble of 2D int8 Metropolis lattices L x L, L/2 x L/2 (four each) and L/4 x L/4
 (sixteen) at temperatures 2.0 .. 2.6, device seeded starts, SWEEPS sweeps with (M, E) every 10,
-through the batched kernel.  Prints the final exact (M, E) (batch: of the first lattice).
+through the batched kernel; batch1: one 2D int8 Metropolis lattice L x L at beta_c alone in a
+batch, device seeded start, no measurement.  Prints the final exact (M, E) (batch: of the first
+lattice).
 """
 
 from __future__ import annotations
@@ -43,6 +45,15 @@ def main(argv: list[str]) -> int:
             ens.run()
             series = ens.result(ids[0]).series
         print(which, L, n, tuple(int(x) for x in series[-1]) if len(series) else None)
+        return 0
+    elif which == "batch1":
+        from .ensemble import Ensemble, Job
+
+        with Ensemble() as ens:
+            i = ens.add(Job((L, L), BETA_C_2D, n, seed=7, init="philox", keep_lattice=True))
+            ens.run()
+            lat = ens.result(i).lattice
+        print(which, L, n, int(lat.astype("int64").sum()))
         return 0
     else:
         raise SystemExit(f"unknown case {which!r}")
