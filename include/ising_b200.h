@@ -330,6 +330,12 @@ int ising_slab_fill_philox(ising_slab* s, uint64_t start_seed);
  * ISING_SLAB_HALO_* / ISING_SLAB_EDGE_*); the region is contiguous and the same size on every
  * slab of a lattice. */
 int ising_slab_halo(ising_slab* s, int color, int which, void** ptr, int64_t* bytes);
+/* Read the neighbouring slab n's edge rows in place instead of this slab's halos: side 0 = the
+ * previous slab (its last rows become this slab's low halo), 1 = the next one (periodic); NULL
+ * goes back to the own halos.  Both must be slabs of the same lattice; on another device, peer
+ * access is enabled (NVLink loads).  No copy is made: the caller orders each half-sweep after the
+ * neighbours' previous half-sweeps (one stream, or events), and keeps n alive while it is set. */
+int ising_slab_set_peer(ising_slab* s, int side, ising_slab* n);
 /* Zero `pairs` (M, E) slots on the device (allocating them on first use). */
 int ising_slab_series_reset(ising_slab* s, int64_t pairs);
 /* One half-sweep of colour `color` at sweep counter t on the slab's stream; with slot >= 0 the

@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "ising_slab_fill_cold": (I, [P]),
     "ising_slab_fill_philox": (I, [P, U64]),
     "ising_slab_halo": (I, [P, I, I, ctypes.POINTER(P), PI64]),
+    "ising_slab_set_peer": (I, [P, I, P]),
     "ising_slab_series_reset": (I, [P, I64]),
     "ising_slab_half_sweep": (I, [P, I, U64, I64]),
     "ising_slab_series_read": (I, [P, I64, P]),

@@ -157,10 +157,13 @@ __device__ __forceinline__ void call_levels(const u32x4& r, const uint4& m, u32 
 
 // Where a lattice piece sits in a bigger lattice (slab decomposition): the Philox word index is
 // w0 + the local word index and the row parity that of the global row (par0 + local row); rows
-// -1 and `rows` are halo rows, not wrapped.  Unused (and compiled out) for whole lattices.
+// -1 and `rows` are not wrapped but read from lo and hi (the slab's halo rows, or a neighbouring
+// slab's edge rows in place).  Unused (and compiled out) for whole lattices.
 struct SlabOffset {
     long long w0;
     int par0;
+    const u64* lo;
+    const u64* hi;
 };
 
 // Global words of one intake batch (one per lane), loaded ahead of use.
@@ -172,7 +175,7 @@ struct IntakeLoads {
 template <bool SLAB = false>
 __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool valid, int nw,
                                             int nw_shift, IntakeLoads& L,
-                                            const SlabOffset& so = SlabOffset{0, 0})
+                                            const SlabOffset& so = {0, 0, nullptr, nullptr})
 {
     if (!valid) {
         L.o = L.c = L.side = L.up = L.dn = 0;
@@ -195,8 +198,8 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
     const int xs = ((py + (int)p.color) & 1) ? (x + 1 == nw ? 0 : x + 1) : (x == 0 ? nw - 1 : x - 1);
     L.side = __ldg(orow + xs);
     if constexpr (SLAB) {
-        L.up = __ldg(orow - nw + x);  // row -1 is the low halo
-        L.dn = __ldg(orow + nw + x);  // row `rows` is the high halo
+        L.up = __ldg((y == 0 ? so.lo : orow - nw) + x);
+        L.dn = __ldg((y + 1 == p.rows ? so.hi : orow + nw) + x);
     } else {
         L.up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
         L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
@@ -209,7 +212,7 @@ template <bool SLAB = false>
 __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begin, long long end,
                                                 int nw_shift, QueueSlots& q,
                                                 const uint4* lvmask,
-                                                const SlabOffset& so = SlabOffset{0, 0})
+                                                const SlabOffset& so = {0, 0, nullptr, nullptr})
 {
     const u32 wg = SLAB ? (u32)so.w0 : 0u;  // Philox word index = wg + local index (mod 2^32)
     const int lane = threadIdx.x & 31;

@@ -48,8 +48,18 @@ struct ising_slab {
     int sm_count = 148;
     int max_blocks = 148 * 8;
     int queue_blocks = 2;  // resident blocks per SM of the msc work-stack kernel
+    // Neighbouring slabs whose edge rows the kernels read in place of this slab's halos
+    // (ising_slab_set_peer), per colour; nullptr: the own halo rows.
+    const char* peer_lo[2] = {nullptr, nullptr};
+    const char* peer_hi[2] = {nullptr, nullptr};
 
     char* owned(int c) const { return static_cast<char*>(base[c]) + halo * row_bytes; }
+    // Where the kernels read the rows before and after the owned ones, in colour c.
+    const char* low_rows(int c) const { return peer_lo[c] ? peer_lo[c] : owned(c) - halo * row_bytes; }
+    const char* high_rows(int c) const
+    {
+        return peer_hi[c] ? peer_hi[c] : owned(c) + rows * (long long)row_bytes;
+    }
 };
 
 namespace ising {
@@ -57,6 +67,9 @@ namespace ising {
 struct SlabGeo {
     long long row0;  // global row of local row 0: the Philox site index is (row0 + row) * lh + j
     int par0;        // parity of the slab's first global y (2D) or z (3D)
+    long long halo;  // rows before (and after) the owned ones that a half-sweep reads
+    const void* lo;  // those rows of the opposite colour: rows -halo .. -1
+    const void* hi;  // and rows `rows` .. rows + halo - 1
 };
 
 // int8 half-sweep of a slab: the band schedule of int8_half_kernel, with the rows next to the
@@ -91,18 +104,25 @@ __global__ void __launch_bounds__(256, 4) int8_slab_kernel(const Int8Half p_in, 
         const int wv = valid_words<true, W>(p, j0);
         const long long plane = (long long)z * ly;
         const int8_t* oth = p.other + j0;
+        const int8_t* lo = static_cast<const int8_t*>(g.lo) + j0;
+        const int8_t* hi = static_cast<const int8_t*>(g.hi) + j0;
+        // opposite-colour row r: rows -halo .. -1 from lo, rows .. rows + halo - 1 from hi
+        auto orow = [&](long long r) -> const int8_t* {
+            return r < 0 ? lo + (r + g.halo) * p.pitch
+                         : (r >= p.rows ? hi + (r - p.rows) * p.pitch : oth + r * p.pitch);
+        };
         // 2D: y is the slab axis, rows -1 and ly are halo rows; 3D: y wraps inside its plane
         const long long yprev = NDIM == 2 ? y0 - 1 : (y0 == 0 ? ly - 1 : y0 - 1);
-        Words<W> nd = load_words_ro<W>(oth + (plane + yprev) * p.pitch);
+        Words<W> nd = load_words_ro<W>(orow(plane + yprev));
         Words<W> c = load_words_ro<W>(oth + (plane + y0) * p.pitch);
         for (int y = y0; y < y1; ++y) {
             const long long row = plane + y;
             const long long ynext = NDIM == 2 ? y + 1 : (y + 1 == ly ? 0 : y + 1);
-            const Words<W> nu = load_words_ro<W>(oth + (plane + ynext) * p.pitch);
+            const Words<W> nu = load_words_ro<W>(orow(plane + ynext));
             Words<W> zu = nu, zd = nd;
             if constexpr (NDIM == 3) {  // planes z +- 1: plane -1 and plane lz are the halos
-                zu = load_words_ro<W>(oth + (row + ly) * p.pitch);
-                zd = load_words_ro<W>(oth + (row - ly) * p.pitch);
+                zu = load_words_ro<W>(orow(row + ly));
+                zd = load_words_ro<W>(orow(row - ly));
             }
             const int par = (g.par0 + y + z + (int)p.color) & 1;
             const u32 edge =
@@ -137,8 +157,8 @@ __global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const Sl
         if ((g.par0 + (int)(y & 1) + (int)p.color) & 1)
             hz = (c >> 1) | (__ldg(orow + (x + 1 == nw ? 0 : x + 1)) << 63);
         else hz = (c << 1) | (__ldg(orow + (x == 0 ? nw - 1 : x - 1)) >> 63);
-        const u64 up = __ldg(orow - nw + x);
-        const u64 dn = __ldg(orow + nw + x);
+        const u64 up = __ldg((y == 0 ? static_cast<const u64*>(g.lo) : orow - nw) + x);
+        const u64 dn = __ldg((y + 1 == p.rows ? static_cast<const u64*>(g.hi) : orow + nw) + x);
         u64 ns = o;
         if constexpr (UPDATE) {
             const Slices s = slice4(o, c, hz, up, dn);
@@ -254,7 +274,8 @@ static void launch_int8_slab_rule(int rule, const Int8Half& p, const SlabGeo& g,
 // One half-sweep of colour `color` (rule kObserve: measurement of colour `color` only).
 static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long long* meas)
 {
-    const SlabGeo g{s->row0, (int)(s->begin & 1)};
+    const SlabGeo g{s->row0, (int)(s->begin & 1), s->halo, s->low_rows(1 - color),
+                    s->high_rows(1 - color)};
     if (s->variant == ISING_VARIANT_MSC) {
         MscHalf p;
         memset(&p, 0, sizeof p);
@@ -272,8 +293,11 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
         p.nw_magic = magic_for(s->nw);
         if (rule != kObserve && !meas) {
             const cudaError_t e = launch_msc_slab_queue(
-                p, SlabOffset{s->row0 * s->nw, (int)(s->begin & 1)}, s->sm_count,
-                s->queue_blocks, s->stream);
+                p,
+                SlabOffset{s->row0 * s->nw, (int)(s->begin & 1),
+                           reinterpret_cast<const u64*>(s->low_rows(1 - color)),
+                           reinterpret_cast<const u64*>(s->high_rows(1 - color))},
+                s->sm_count, s->queue_blocks, s->stream);
             return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
         }
         const unsigned grid = slab_grid(s->rows * (long long)s->nw, s->max_blocks);
@@ -536,6 +560,43 @@ int ising_slab_halo(ising_slab* s, int color, int which, void** ptr, int64_t* by
     default: return fail(ISING_ERR_INVALID, "unknown halo selector %d", which);
     }
     *bytes = hb;
+    return ISING_OK;
+}
+
+int ising_slab_set_peer(ising_slab* s, int side, ising_slab* n)
+{
+    SLAB_CHECK(s);
+    if (side != 0 && side != 1) return fail(ISING_ERR_INVALID, "side must be 0 (low) or 1 (high)");
+    if (!n) {
+        for (int c = 0; c < 2; ++c) (side ? s->peer_hi : s->peer_lo)[c] = nullptr;
+        return ISING_OK;
+    }
+    bool same = n->variant == s->variant && n->ndim == s->ndim && n->row_bytes == s->row_bytes &&
+                n->halo == s->halo && n->lh == s->lh;
+    for (int i = 0; i < 3; ++i) same = same && n->shape[i] == s->shape[i];
+    if (!same) return fail(ISING_ERR_INVALID, "peer slab of a different lattice");
+    const int64_t extent = s->shape[0];
+    const bool adjacent = side == 0 ? (n->begin + n->count) % extent == s->begin
+                                    : (s->begin + s->count) % extent == n->begin;
+    if (!adjacent)
+        return fail(ISING_ERR_INVALID, "peer slab [%lld, %lld) is not the %s neighbour of [%lld, %lld)",
+                    (long long)n->begin, (long long)(n->begin + n->count), side ? "high" : "low",
+                    (long long)s->begin, (long long)(s->begin + s->count));
+    if (n->device != s->device) {
+        int can = 0;
+        SLAB_TRY(cudaDeviceCanAccessPeer(&can, s->device, n->device));
+        if (!can)
+            return fail(ISING_ERR_INVALID, "device %d cannot read device %d's memory", s->device,
+                        n->device);
+        SLAB_TRY(cudaSetDevice(s->device));
+        const cudaError_t e = cudaDeviceEnablePeerAccess(n->device, 0);
+        if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+        else if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceEnablePeerAccess");
+    }
+    for (int c = 0; c < 2; ++c) {
+        if (side == 0) s->peer_lo[c] = n->owned(c) + (n->rows - n->halo) * (long long)n->row_bytes;
+        else s->peer_hi[c] = n->owned(c);
+    }
     return ISING_OK;
 }
 

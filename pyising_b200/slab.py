@@ -9,10 +9,13 @@ wrapping.  Random numbers are keyed by global site index, sweep and colour, so t
 together give exactly the spins and (M, E) series of one GPU running the whole lattice (and of
 pyising's NumPy backend, src/pyising/backends/numpy_backend.py:26-124).
 
-Two exchanges:
+Three exchanges:
 
-* :class:`LocalExchange`: every slab in this process (several GPUs of one process, or several
-  slabs on one GPU); halos are filled by device copies (peer copies between GPUs).
+* :class:`PeerExchange` (the default within one process): every slab in this process (several
+  GPUs of one process, or several slabs on one GPU); no copies: the kernels read the
+  neighbouring slabs' edge rows in place, over NVLink between GPUs, ordered by CUDA events.
+* :class:`LocalExchange`: the same slabs, halos filled by device copies (peer copies between
+  GPUs).
 * :class:`RingExchange`: one slab per rank of a ``torch.distributed`` process group, ranks in
   slab order; each exchange is one batch of two sends and two receives to the neighbouring
   ranks (NCCL over NVLink on GPUs, gloo on CPU), and (M, E) sums are one int64 all-reduce.
@@ -142,6 +145,12 @@ class Slab:
                                                  device=f"cuda:{self.device}")
         return self._regions[key]
 
+    def set_peer(self, side: int, other: Slab | None) -> None:
+        """Read ``other``'s edge rows in place of this slab's halos (side 0: the previous slab,
+        1: the next one); ``None``: back to the own halos."""
+        check(lib().ising_slab_set_peer(self._h, int(side), other._h if other is not None
+                                        else None), "slab_set_peer")
+
     def half_sweep(self, colour: int, t: int, slot: int = -1) -> None:
         check(lib().ising_slab_half_sweep(self._h, colour, int(t), int(slot)), "slab_half_sweep")
 
@@ -172,6 +181,42 @@ class LocalExchange:
         for i, s in enumerate(slabs):
             s.region(colour, HALO_LOW).copy_(slabs[i - 1].region(colour, EDGE_HIGH))
             s.region(colour, HALO_HIGH).copy_(slabs[(i + 1) % n].region(colour, EDGE_LOW))
+
+    def allreduce(self, values: np.ndarray) -> np.ndarray:
+        return values
+
+
+class PeerExchange:
+    """All slabs of the lattice in this process, in slab order, with no halo copies at all: each
+    slab's kernels read its neighbours' edge rows in place (NVLink peer loads between GPUs, set
+    up once by ``Slab.set_peer``).  An exchange only orders the work: every slab's next
+    half-sweep waits for its neighbours' last half-sweeps (CUDA events across streams), which
+    both makes their edges current (read after write) and keeps them from being rewritten while
+    they are still read (write after read).  Slabs on one stream need nothing."""
+
+    def __init__(self, slabs, streams=None) -> None:
+        n = len(slabs)
+        for i, s in enumerate(slabs):
+            s.set_peer(0, slabs[i - 1])
+            s.set_peer(1, slabs[(i + 1) % n])
+        self.streams = list(streams) if streams is not None else None
+
+    def exchange(self, slabs, colour: int) -> None:
+        st = self.streams
+        if st is None or all(x is st[0] for x in st):
+            return
+        import torch
+
+        events = []
+        for x in st:
+            ev = torch.cuda.Event()
+            ev.record(x)
+            events.append(ev)
+        n = len(slabs)
+        for i, x in enumerate(st):
+            for j in (i - 1, (i + 1) % n):
+                if st[j % n] is not x:
+                    x.wait_event(events[j % n])
 
     def allreduce(self, values: np.ndarray) -> np.ndarray:
         return values
@@ -305,14 +350,16 @@ class SlabSimulation:
     ``group``: a ``torch.distributed`` process group (or ``"default"`` for the default one),
     one slab per rank on this rank's current CUDA device, NCCL halos (:class:`RingExchange`).
     Otherwise every slab lives in this process: ``parts`` slabs (default: one per GPU) on
-    ``devices`` (default: all GPUs, round robin), device-copy halos (:class:`LocalExchange`).
+    ``devices`` (default: all GPUs, round robin), the kernels reading their neighbours' edge rows
+    in place (``exchange="peer"``, :class:`PeerExchange`) or from halo copies
+    (``exchange="copy"``, :class:`LocalExchange`).
     ``init``: ``"hot"`` (NumPy's PCG64 start of pyising, generated on every rank), ``"cold"``,
     ``"philox"`` (the device seeded start, no host work) or a full int8 lattice.
     """
 
     def __init__(self, shape, beta: float, seed: int = 0, algorithm: str = "metropolis",
                  variant: str = "int8", init="hot", *, parts: int | None = None,
-                 devices=None, group=None) -> None:
+                 devices=None, group=None, exchange: str = "peer") -> None:
         import torch
 
         if variant not in ("int8", "msc"):
@@ -338,7 +385,7 @@ class SlabSimulation:
             dev = torch.cuda.current_device()
             self.slabs = [Slab(self.shape, self.table, self.seed, algorithm, variant,
                                *ranges[rank], device=dev)]
-            exchange = RingExchange(g, device=f"cuda:{dev}")
+            ring = RingExchange(g, device=f"cuda:{dev}")
         else:
             ndev = torch.cuda.device_count()
             devices = list(devices) if devices is not None else list(range(ndev))
@@ -347,13 +394,19 @@ class SlabSimulation:
             self.slabs = [Slab(self.shape, self.table, self.seed, algorithm, variant, b, c,
                                device=devices[i % len(devices)])
                           for i, (b, c) in enumerate(ranges)]
-            exchange = LocalExchange()
+            if exchange not in ("peer", "copy"):
+                raise ValueError(f"unknown exchange {exchange!r}")
         streams = {}
         for s in self.slabs:
             if s.device not in streams:
                 streams[s.device] = torch.cuda.Stream(device=s.device)
             s.set_stream(streams[s.device].cuda_stream)
-        self.runner = SlabRunner(self.slabs, exchange, streams=list(streams.values()))
+        if group is None:
+            ex = (PeerExchange(self.slabs, [streams[s.device] for s in self.slabs])
+                  if exchange == "peer" else LocalExchange())
+        else:
+            ex = ring
+        self.runner = SlabRunner(self.slabs, ex, streams=list(streams.values()))
         if isinstance(init, np.ndarray):
             self.set_lattice(init)
         elif init == "hot":
@@ -443,5 +496,18 @@ class SlabSimulation:
             s.sync()
 
     def close(self) -> None:
-        for s in self.slabs:
+        """Frees the slabs, after every stream's work is done (with peer reads a slab's memory
+        may be read by its neighbours' kernels on other streams)."""
+        slabs = getattr(self, "slabs", [])
+        for s in slabs:
+            if s._h is not None and s._h.value:
+                s.sync()
+        for s in slabs:
             s.close()
+        self.slabs = []
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

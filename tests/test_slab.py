@@ -262,8 +262,9 @@ GPU_CASES = [
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("exchange", ["peer", "copy"])
 @pytest.mark.parametrize("variant,shape,algorithm,beta,parts", GPU_CASES)
-def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts):
+def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts, exchange):
     from pyising_b200.backend import B200Int8, B200MultiSpin
     from pyising_b200.slab import SlabSimulation
 
@@ -271,7 +272,7 @@ def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts):
     one_cls = B200MultiSpin if variant == "msc" else B200Int8
     one = one_cls(shape, beta, seed=seed, algorithm=algorithm, init="hot")
     split = SlabSimulation(shape, beta, seed=seed, algorithm=algorithm, variant=variant,
-                           init="hot", parts=parts, devices=[0])
+                           init="hot", parts=parts, devices=[0], exchange=exchange)
     np.testing.assert_array_equal(split.get_lattice(), one.get_lattice())
     want = one.sweep_measured(12, 3)
     got = split.sweep_measured(12, 3)
@@ -321,7 +322,18 @@ def test_gpu_slab_argument_errors():
         s.half_sweep(0, 0, slot=0)  # no series reset
     with pytest.raises(ValueError):
         s.half_sweep(2, 0)
-    s.close()
+    far = Slab((16, 16), tab, 0, "metropolis", "int8", 12, 4)
+    other = Slab((16, 32), tab, 0, "metropolis", "int8", 0, 4)
+    with pytest.raises(ValueError):
+        s.set_peer(0, far)  # [12, 16) is not the low neighbour of [4, 8)
+    with pytest.raises(ValueError):
+        s.set_peer(1, other)  # another lattice
+    with pytest.raises(ValueError):
+        s.set_peer(2, far)
+    s.set_peer(1, Slab((16, 16), tab, 0, "metropolis", "int8", 8, 8))
+    s.set_peer(1, None)
+    for x in (s, far, other):
+        x.close()
 
 
 def _nccl_world1_worker(port, queue):
