@@ -85,6 +85,8 @@ __global__ void __launch_bounds__(256, 4) int8_slab_kernel(const Int8Half p_in, 
 #pragma unroll
         for (int i = 0; i < 7; ++i) stab[i] = p.table[i];
     }
+    pdl_wait();  // the previous kernel of the stream has completed
+    pdl_trigger();
     __syncthreads();
     long long m_acc = 0, e_acc = 0;
     const u32 cpr = (u32)p.cpr, bpp = (u32)p.bpp;
@@ -142,6 +144,8 @@ __global__ void __launch_bounds__(256, 4) int8_slab_kernel(const Int8Half p_in, 
 template <bool UPDATE, bool MEAS>
 __global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const SlabGeo g)
 {
+    pdl_wait();
+    pdl_trigger();
     long long m_acc = 0, e_acc = 0;
     const int nw = p.nw;
     const long long words = (long long)p.rows * nw;
@@ -188,6 +192,8 @@ __global__ void __launch_bounds__(kSlabQueueWarps * 32)
     __shared__ QueueSlots q_all[kSlabQueueWarps];
     __shared__ uint4 lvmask[16];
     if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+    pdl_wait();
+    pdl_trigger();
     __syncthreads();
     const long long begin =
         ((long long)blockIdx.x * kSlabQueueWarps + (threadIdx.x >> 5)) * per_warp;
@@ -205,8 +211,8 @@ static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so,
     const long long nwarps = (total + per_warp - 1) / per_warp;
     const unsigned blocks = (unsigned)((nwarps + kSlabQueueWarps - 1) / kSlabQueueWarps);
     const int shift = (p.nw & (p.nw - 1)) == 0 ? __builtin_ctz((unsigned)p.nw) : -1;
-    msc_slab_queue_kernel<<<blocks, kSlabQueueWarps * 32, 0, st>>>(p, so, total, per_warp, shift);
-    return cudaGetLastError();
+    return launch_pdl(msc_slab_queue_kernel, dim3(blocks), dim3(kSlabQueueWarps * 32), st, p, so,
+                      total, per_warp, shift);
 }
 
 // The device seeded start of ising_fill_philox at global site indices.
@@ -258,16 +264,13 @@ template <int NDIM, bool MEAS>
 static void launch_int8_slab_rule(int rule, const Int8Half& p, const SlabGeo& g, unsigned grid,
                                   cudaStream_t st)
 {
+    auto go = [&](auto kernel) { launch_pdl(kernel, dim3(grid), dim3(256), st, p, g); };
     switch (rule) {
-    case kMetroFast: int8_slab_kernel<NDIM, kMetroFast, MEAS><<<grid, 256, 0, st>>>(p, g); break;
-    case kHeatFast: int8_slab_kernel<NDIM, kHeatFast, MEAS><<<grid, 256, 0, st>>>(p, g); break;
-    case kMetroGeneric:
-        int8_slab_kernel<NDIM, kMetroGeneric, MEAS><<<grid, 256, 0, st>>>(p, g);
-        break;
-    case kHeatGeneric:
-        int8_slab_kernel<NDIM, kHeatGeneric, MEAS><<<grid, 256, 0, st>>>(p, g);
-        break;
-    default: int8_slab_kernel<NDIM, kObserve, true><<<grid, 256, 0, st>>>(p, g); break;
+    case kMetroFast: go(int8_slab_kernel<NDIM, kMetroFast, MEAS>); break;
+    case kHeatFast: go(int8_slab_kernel<NDIM, kHeatFast, MEAS>); break;
+    case kMetroGeneric: go(int8_slab_kernel<NDIM, kMetroGeneric, MEAS>); break;
+    case kHeatGeneric: go(int8_slab_kernel<NDIM, kHeatGeneric, MEAS>); break;
+    default: go(int8_slab_kernel<NDIM, kObserve, true>); break;
     }
 }
 
@@ -301,9 +304,10 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
             return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
         }
         const unsigned grid = slab_grid(s->rows * (long long)s->nw, s->max_blocks);
-        if (rule == kObserve) msc_slab_kernel<false, true><<<grid, 256, 0, s->stream>>>(p, g);
-        else if (meas) msc_slab_kernel<true, true><<<grid, 256, 0, s->stream>>>(p, g);
-        else msc_slab_kernel<true, false><<<grid, 256, 0, s->stream>>>(p, g);
+        auto go = [&](auto kernel) { launch_pdl(kernel, dim3(grid), dim3(256), s->stream, p, g); };
+        if (rule == kObserve) go(msc_slab_kernel<false, true>);
+        else if (meas) go(msc_slab_kernel<true, true>);
+        else go(msc_slab_kernel<true, false>);
     } else {
         Int8Half p;
         memset(&p, 0, sizeof p);
