@@ -1,6 +1,6 @@
 """Run one small sweep case, for profilers (ncu) and quick timing.
 
-    python -m pyising_b200.profile_case {int8|hb3|msc|sw|batch|batch1} L SWEEPS
+    python -m pyising_b200.profile_case {int8|hb3|msc|sw|batch|batch1|slab2|mscslab2} L SWEEPS
 
 int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
 beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start seed 7;
@@ -8,8 +8,9 @@ sw: SWEEPS Swendsen-Wang updates of a 2D int8 L x L lattice at beta_c from a col
 batch: an ensemble of 2D int8 Metropolis lattices L x L, L/2 x L/2 (four each) and L/4 x L/4
 (sixteen) at temperatures 2.0 .. 2.6, device seeded starts, SWEEPS sweeps with (M, E) every 10,
 through the batched kernel; batch1: one 2D int8 Metropolis lattice L x L at beta_c alone in a
-batch, device seeded start, no measurement.  Prints the final exact (M, E) (batch: of the first
-lattice).
+batch, device seeded start, no measurement; slab2 / mscslab2: a 2D int8 / msc Metropolis L x L
+lattice at beta_c cut into two slabs on device 0 (neighbour rows read in place), device seeded
+start.  Prints the final exact (M, E) (batch: of the first lattice).
 """
 
 from __future__ import annotations
@@ -45,6 +46,16 @@ def main(argv: list[str]) -> int:
             ens.run()
             series = ens.result(ids[0]).series
         print(which, L, n, tuple(int(x) for x in series[-1]) if len(series) else None)
+        return 0
+    elif which in ("slab2", "mscslab2"):
+        from .slab import SlabSimulation
+
+        sim = SlabSimulation((L, L), BETA_C_2D, seed=7, variant="msc" if which == "mscslab2"
+                             else "int8", init="philox", parts=2, devices=[0])
+        sim.sweep(n)
+        sim.synchronize()
+        print(which, L, n, sim.observables_int())
+        sim.close()
         return 0
     elif which == "batch1":
         from .ensemble import Ensemble, Job
