@@ -342,6 +342,11 @@ int ising_slab_series_reset(ising_slab* s, int64_t pairs);
  * half-sweep also adds the slab's exact (M, E) after it to series slot `slot` (measure on
  * colour 1, the second half of a sweep, as ising_sweep does). */
 int ising_slab_half_sweep(ising_slab* s, int color, uint64_t t, int64_t slot);
+/* The same over rows (2D) or planes (3D) first .. first + count - 1 of the slab only: the rows
+ * that read no halo (all but the first and the last) can run while the halos are still being
+ * exchanged, the two edge rows after it. */
+int ising_slab_half_sweep_rows(ising_slab* s, int color, uint64_t t, int64_t slot, int64_t first,
+                               int64_t count);
 /* Copy `pairs` series slots to the host (blocks). */
 int ising_slab_series_read(ising_slab* s, int64_t pairs, int64_t* out);
 /* The slab's (M, E) over its owned sites (blocks); the colour-0 halos must be current. */

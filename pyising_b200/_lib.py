@@ -84,6 +84,7 @@ SIGNATURES: dict[str, tuple] = {
     "ising_slab_set_peer": (I, [P, I, P]),
     "ising_slab_series_reset": (I, [P, I64]),
     "ising_slab_half_sweep": (I, [P, I, U64, I64]),
+    "ising_slab_half_sweep_rows": (I, [P, I, U64, I64, I64, I64]),
     "ising_slab_series_read": (I, [P, I64, P]),
     "ising_slab_observables": (I, [P, PI64, PI64]),
     "ising_slab_sync": (I, [P]),

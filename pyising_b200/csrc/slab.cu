@@ -70,6 +70,7 @@ struct SlabGeo {
     long long halo;  // rows before (and after) the owned ones that a half-sweep reads
     const void* lo;  // those rows of the opposite colour: rows -halo .. -1
     const void* hi;  // and rows `rows` .. rows + halo - 1
+    int a0, an;      // the launch updates rows (2D) or planes (3D) a0 .. a0 + an - 1
 };
 
 // int8 half-sweep of a slab: the band schedule of int8_half_kernel, with the rows next to the
@@ -90,19 +91,22 @@ __global__ void __launch_bounds__(256, 4) int8_slab_kernel(const Int8Half p_in, 
     __syncthreads();
     long long m_acc = 0, e_acc = 0;
     const u32 cpr = (u32)p.cpr, bpp = (u32)p.bpp;
-    const u32 nslots = (u32)p.lz * bpp * cpr;
+    // bands over rows a0 .. a0 + an - 1 (2D) or over all rows of planes a0 .. a0 + an - 1 (3D)
+    const u32 nslots = (u32)(NDIM == 3 ? g.an : 1) * bpp * cpr;
     const int ly = p.ly;
+    const int ybase = NDIM == 2 ? g.a0 : 0, yend = NDIM == 2 ? g.a0 + g.an : ly;
     for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
          slot += gridDim.x * blockDim.x) {
         const u32 band = fast_div(slot, cpr, p.cpr_magic);
         const int j0 = (int)(slot - band * cpr) * V;
         int z = 0, yb = (int)band;
         if constexpr (NDIM == 3) {
-            z = (int)fast_div(band, bpp, p.bpp_magic);
-            yb = (int)(band - (u32)z * bpp);
+            const int zs = (int)fast_div(band, bpp, p.bpp_magic);
+            yb = (int)(band - (u32)zs * bpp);
+            z = g.a0 + zs;
         }
-        const int y0 = yb * p.band;
-        const int y1 = y0 + p.band < ly ? y0 + p.band : ly;
+        const int y0 = ybase + yb * p.band;
+        const int y1 = y0 + p.band < yend ? y0 + p.band : yend;
         const int wv = valid_words<true, W>(p, j0);
         const long long plane = (long long)z * ly;
         const int8_t* oth = p.other + j0;
@@ -148,9 +152,9 @@ __global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const Sl
     pdl_trigger();
     long long m_acc = 0, e_acc = 0;
     const int nw = p.nw;
-    const long long words = (long long)p.rows * nw;
-    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < words;
-         w += (long long)gridDim.x * blockDim.x) {
+    const long long w_end = (long long)(g.a0 + g.an) * nw;
+    for (long long w = (long long)g.a0 * nw + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         w < w_end; w += (long long)gridDim.x * blockDim.x) {
         const long long y = w / nw;
         const int x = (int)(w - y * nw);
         const long long rb = y * nw;
@@ -186,8 +190,8 @@ __global__ void __launch_bounds__(256) msc_slab_kernel(const MscHalf p, const Sl
 constexpr int kSlabQueueWarps = 8;
 
 __global__ void __launch_bounds__(kSlabQueueWarps * 32)
-    msc_slab_queue_kernel(const MscHalf p, const SlabOffset so, long long total,
-                          long long per_warp, int nw_shift)
+    msc_slab_queue_kernel(const MscHalf p, const SlabOffset so, long long first,
+                          long long total, long long per_warp, int nw_shift)
 {
     __shared__ QueueSlots q_all[kSlabQueueWarps];
     __shared__ uint4 lvmask[16];
@@ -198,13 +202,15 @@ __global__ void __launch_bounds__(kSlabQueueWarps * 32)
     const long long begin =
         ((long long)blockIdx.x * kSlabQueueWarps + (threadIdx.x >> 5)) * per_warp;
     const long long end = begin + per_warp < total ? begin + per_warp : total;
-    msc_queue_range<true>(p, begin, end, nw_shift, q_all[threadIdx.x >> 5], lvmask, so);
+    msc_queue_range<true>(p, first + begin, first + end, nw_shift, q_all[threadIdx.x >> 5],
+                          lvmask, so);
 }
 
-static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so, int sm_count,
-                                         int blocks_per_sm, cudaStream_t st)
+// Words a0 * nw .. (a0 + an) * nw - 1 (rows a0 .. a0 + an - 1).
+static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so, int a0, int an,
+                                         int sm_count, int blocks_per_sm, cudaStream_t st)
 {
-    const long long total = (long long)p.rows * p.nw;
+    const long long total = (long long)an * p.nw;
     const long long warps = (long long)sm_count * blocks_per_sm * kSlabQueueWarps;
     long long per_warp = (total + warps - 1) / warps;
     per_warp = (per_warp + 31) / 32 * 32;
@@ -212,7 +218,7 @@ static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so,
     const unsigned blocks = (unsigned)((nwarps + kSlabQueueWarps - 1) / kSlabQueueWarps);
     const int shift = (p.nw & (p.nw - 1)) == 0 ? __builtin_ctz((unsigned)p.nw) : -1;
     return launch_pdl(msc_slab_queue_kernel, dim3(blocks), dim3(kSlabQueueWarps * 32), st, p, so,
-                      total, per_warp, shift);
+                      (long long)a0 * p.nw, total, per_warp, shift);
 }
 
 // The device seeded start of ising_fill_philox at global site indices.
@@ -274,11 +280,13 @@ static void launch_int8_slab_rule(int rule, const Int8Half& p, const SlabGeo& g,
     }
 }
 
-// One half-sweep of colour `color` (rule kObserve: measurement of colour `color` only).
-static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long long* meas)
+// One half-sweep of colour `color` (rule kObserve: measurement of colour `color` only) over
+// rows (2D) or planes (3D) a0 .. a0 + an - 1 of the slab.
+static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long long* meas, int a0,
+                     int an)
 {
     const SlabGeo g{s->row0, (int)(s->begin & 1), s->halo, s->low_rows(1 - color),
-                    s->high_rows(1 - color)};
+                    s->high_rows(1 - color), a0, an};
     if (s->variant == ISING_VARIANT_MSC) {
         MscHalf p;
         memset(&p, 0, sizeof p);
@@ -300,10 +308,10 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
                 SlabOffset{s->row0 * s->nw, (int)(s->begin & 1),
                            reinterpret_cast<const u64*>(s->low_rows(1 - color)),
                            reinterpret_cast<const u64*>(s->high_rows(1 - color))},
-                s->sm_count, s->queue_blocks, s->stream);
+                a0, an, s->sm_count, s->queue_blocks, s->stream);
             return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
         }
-        const unsigned grid = slab_grid(s->rows * (long long)s->nw, s->max_blocks);
+        const unsigned grid = slab_grid((long long)an * s->nw, s->max_blocks);
         auto go = [&](auto kernel) { launch_pdl(kernel, dim3(grid), dim3(256), s->stream, p, g); };
         if (rule == kObserve) go(msc_slab_kernel<false, true>);
         else if (meas) go(msc_slab_kernel<true, true>);
@@ -326,7 +334,16 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
         p.k1 = (u32)(s->seed >> 32);
         for (int i = 0; i < 7; ++i) p.table[i] = s->table[i];
         p.meas = meas;
-        const unsigned grid = int8_band_geometry(p, s->max_blocks, s->sm_count);
+        // band geometry of the updated range; the kernel keeps the slab's own extents
+        Int8Half q = p;
+        if (s->ndim == 2) q.ly = an;
+        else q.lz = an;
+        q.rows = (long long)q.ly * q.lz;
+        const unsigned grid = int8_band_geometry(q, s->max_blocks, s->sm_count);
+        p.band = q.band;
+        p.bpp = q.bpp;
+        p.cpr_magic = q.cpr_magic;
+        p.bpp_magic = q.bpp_magic;
         const bool m = meas != nullptr;
         if (s->ndim == 3) {
             if (m) launch_int8_slab_rule<3, true>(rule, p, g, grid, s->stream);
@@ -628,17 +645,28 @@ int ising_slab_series_reset(ising_slab* s, int64_t pairs)
     return ISING_OK;
 }
 
-int ising_slab_half_sweep(ising_slab* s, int color, uint64_t t, int64_t slot)
+int ising_slab_half_sweep_rows(ising_slab* s, int color, uint64_t t, int64_t slot,
+                               int64_t first, int64_t count)
 {
     SLAB_CHECK(s);
     if (color != 0 && color != 1) return fail(ISING_ERR_INVALID, "colour must be 0 or 1");
     if (slot >= s->series_cap)
         return fail(ISING_ERR_INVALID, "series slot %lld beyond the %lld reset pairs",
                     (long long)slot, (long long)s->series_cap);
+    if (first < 0 || count < 0 || first + count > s->count)
+        return fail(ISING_ERR_INVALID, "rows [%lld, %lld) outside the slab's %lld",
+                    (long long)first, (long long)(first + count), (long long)s->count);
+    if (count == 0) return ISING_OK;
     SLAB_TRY(cudaSetDevice(s->device));
     unsigned long long* m =
         slot >= 0 ? reinterpret_cast<unsigned long long*>(s->d_series + 2 * slot) : nullptr;
-    return slab_half(s, color, (u32)t, s->rule, m);
+    return slab_half(s, color, (u32)t, s->rule, m, (int)first, (int)count);
+}
+
+int ising_slab_half_sweep(ising_slab* s, int color, uint64_t t, int64_t slot)
+{
+    SLAB_CHECK(s);
+    return ising_slab_half_sweep_rows(s, color, t, slot, 0, s->count);
 }
 
 int ising_slab_series_read(ising_slab* s, int64_t pairs, int64_t* out)
@@ -662,7 +690,7 @@ int ising_slab_observables(ising_slab* s, int64_t* m, int64_t* e)
     if (!m || !e) return fail(ISING_ERR_INVALID, "null output pointer");
     SLAB_TRY(cudaSetDevice(s->device));
     SLAB_TRY(cudaMemsetAsync(s->d_acc, 0, 2 * sizeof(unsigned long long), s->stream));
-    const int rc = slab_half(s, 1, 0u, kObserve, s->d_acc);
+    const int rc = slab_half(s, 1, 0u, kObserve, s->d_acc, 0, (int)s->count);
     if (rc != ISING_OK) return rc;
     long long out[2];
     SLAB_TRY(cudaMemcpyAsync(out, s->d_acc, sizeof out, cudaMemcpyDeviceToHost, s->stream));

@@ -151,8 +151,13 @@ class Slab:
         check(lib().ising_slab_set_peer(self._h, int(side), other._h if other is not None
                                         else None), "slab_set_peer")
 
-    def half_sweep(self, colour: int, t: int, slot: int = -1) -> None:
-        check(lib().ising_slab_half_sweep(self._h, colour, int(t), int(slot)), "slab_half_sweep")
+    def half_sweep(self, colour: int, t: int, slot: int = -1, first: int = 0,
+                   count: int | None = None) -> None:
+        """Half-sweep of rows (2D) or planes (3D) ``first .. first + count - 1`` (all by
+        default) of the slab."""
+        n = self.count - first if count is None else count
+        check(lib().ising_slab_half_sweep_rows(self._h, colour, int(t), int(slot), int(first),
+                                               int(n)), "slab_half_sweep")
 
     def series_reset(self, pairs: int) -> None:
         check(lib().ising_slab_series_reset(self._h, int(pairs)), "slab_series_reset")
@@ -174,13 +179,22 @@ class Slab:
 
 
 class LocalExchange:
-    """All slabs of the lattice in this process, in slab order: halos filled by device copies."""
+    """All slabs of the lattice in this process, in slab order: halos filled by device copies.
+
+    ``start`` / ``finish`` split an exchange so that work can be issued in between (the slab
+    runner's overlap mode); here the copies are issued by ``start``."""
 
     def exchange(self, slabs, colour: int) -> None:
         n = len(slabs)
         for i, s in enumerate(slabs):
             s.region(colour, HALO_LOW).copy_(slabs[i - 1].region(colour, EDGE_HIGH))
             s.region(colour, HALO_HIGH).copy_(slabs[(i + 1) % n].region(colour, EDGE_LOW))
+
+    def start(self, slabs, colour: int):
+        self.exchange(slabs, colour)
+
+    def finish(self, pending) -> None:
+        pass
 
     def allreduce(self, values: np.ndarray) -> np.ndarray:
         return values
@@ -218,6 +232,12 @@ class PeerExchange:
                 if st[j % n] is not x:
                     x.wait_event(events[j % n])
 
+    def start(self, slabs, colour: int):
+        self.exchange(slabs, colour)
+
+    def finish(self, pending) -> None:
+        pass
+
     def allreduce(self, values: np.ndarray) -> np.ndarray:
         return values
 
@@ -240,10 +260,19 @@ class RingExchange:
         return self.dist.get_global_rank(self.group, r) if self.group is not None else r
 
     def exchange(self, slabs, colour: int) -> None:
+        self.finish(self.start(slabs, colour))
+
+    def finish(self, pending) -> None:
+        for w in pending or ():
+            w.wait()
+
+    def start(self, slabs, colour: int):
+        """Issues the two sends and two receives; ``finish`` waits for them (on GPUs: makes
+        the current stream wait), so that rows reading no halo can be updated in between."""
         (s,) = slabs
         if self.world == 1:
             LocalExchange().exchange(slabs, colour)
-            return
+            return None
         d = self.dist
         prev = self._global((self.rank - 1) % self.world)
         nxt = self._global((self.rank + 1) % self.world)
@@ -254,8 +283,7 @@ class RingExchange:
                d.P2POp(d.isend, s.region(colour, EDGE_HIGH), nxt, self.group, 2 * colour + 1),
                d.P2POp(d.irecv, s.region(colour, HALO_HIGH), nxt, self.group, 2 * colour),
                d.P2POp(d.irecv, s.region(colour, HALO_LOW), prev, self.group, 2 * colour + 1)]
-        for w in d.batch_isend_irecv(ops):
-            w.wait()
+        return d.batch_isend_irecv(ops)
 
     def allreduce(self, values: np.ndarray) -> np.ndarray:
         import torch
@@ -275,11 +303,12 @@ class SlabRunner:
     the loop issues copies and collectives so that they are ordered with the kernels.
     """
 
-    def __init__(self, slabs, exchange, t: int = 0, streams=()) -> None:
+    def __init__(self, slabs, exchange, t: int = 0, streams=(), overlap: bool = False) -> None:
         self.slabs = list(slabs)
         self.exchange = exchange
         self.t = int(t)
         self.streams = list(streams)
+        self.overlap = bool(overlap)
         self._fresh = [False, False]
 
     @contextlib.contextmanager
@@ -317,14 +346,8 @@ class SlabRunner:
                 slot = -1
                 if measure_every > 0 and (i + 1) % measure_every == 0:
                     slot, k = k, k + 1
-                self._refresh(1)
-                for s in self.slabs:
-                    s.half_sweep(0, self.t)
-                self._fresh[0] = False
-                self._refresh(0)
-                for s in self.slabs:
-                    s.half_sweep(1, self.t, slot)
-                self._fresh[1] = False
+                self._half(0, -1)
+                self._half(1, slot)
                 self.t += 1
             if not n_meas:
                 return None
@@ -332,6 +355,27 @@ class SlabRunner:
             for s in self.slabs:
                 local += s.series_read(n_meas)
             return self.exchange.allreduce(local).reshape(n_meas, 2)
+
+    def _half(self, colour: int, slot: int) -> None:
+        """One half-sweep of every slab.  In overlap mode, with halos to refresh and slabs of at
+        least three rows (planes), the rows that read no halo are issued between the start and
+        the finish of the exchange, the first and last row after it."""
+        other = colour ^ 1
+        if (self.overlap and not self._fresh[other] and
+                all(s.count >= 3 for s in self.slabs)):
+            pending = self.exchange.start(self.slabs, other)
+            for s in self.slabs:
+                s.half_sweep(colour, self.t, slot, 1, s.count - 2)
+            self.exchange.finish(pending)
+            self._fresh[other] = True
+            for s in self.slabs:
+                s.half_sweep(colour, self.t, slot, 0, 1)
+                s.half_sweep(colour, self.t, slot, s.count - 1, 1)
+        else:
+            self._refresh(other)
+            for s in self.slabs:
+                s.half_sweep(colour, self.t, slot)
+        self._fresh[colour] = False
 
     def observables_int(self) -> tuple[int, int]:
         """Exact (M, E) of the whole lattice."""
@@ -354,12 +398,15 @@ class SlabSimulation:
     in place (``exchange="peer"``, :class:`PeerExchange`) or from halo copies
     (``exchange="copy"``, :class:`LocalExchange`).
     ``init``: ``"hot"`` (NumPy's PCG64 start of pyising, generated on every rank), ``"cold"``,
-    ``"philox"`` (the device seeded start, no host work) or a full int8 lattice.
+    ``"philox"`` (the device seeded start, no host work) or a full int8 lattice.  ``overlap``
+    (default: with a process group) updates the rows that read no halo while the halos are in
+    flight.
     """
 
     def __init__(self, shape, beta: float, seed: int = 0, algorithm: str = "metropolis",
                  variant: str = "int8", init="hot", *, parts: int | None = None,
-                 devices=None, group=None, exchange: str = "peer") -> None:
+                 devices=None, group=None, exchange: str = "peer",
+                 overlap: bool | None = None) -> None:
         import torch
 
         if variant not in ("int8", "msc"):
@@ -406,7 +453,11 @@ class SlabSimulation:
                   if exchange == "peer" else LocalExchange())
         else:
             ex = ring
-        self.runner = SlabRunner(self.slabs, ex, streams=list(streams.values()))
+        # overlap the exchange with the rows that read no halo: by default between processes,
+        # where the exchange is NCCL traffic (in one process it only adds launches)
+        if overlap is None:
+            overlap = group is not None
+        self.runner = SlabRunner(self.slabs, ex, streams=list(streams.values()), overlap=overlap)
         if isinstance(init, np.ndarray):
             self.set_lattice(init)
         elif init == "hot":

@@ -93,6 +93,7 @@ class CpuSlab:
 
     def __init__(self, lat, begin, count, beta, seed, algorithm):
         shape = lat.shape
+        self.count = count
         self.ndim = len(shape)
         self.ly = shape[1] if self.ndim == 3 else count
         inner = shape[1] if self.ndim == 3 else 1
@@ -117,11 +118,17 @@ class CpuSlab:
               EDGE_LOW: slice(h, 2 * h), EDGE_HIGH: slice(r, h + r)}[which]
         return torch.from_numpy(arr[sl].reshape(-1).view(np.uint8))
 
-    def _field(self, colour):
-        """Sum of the opposite colour's neighbours of every owned site of `colour`."""
-        h, rows, ly, lh = self.halo, self.rows, self.ly, self.lh
+    def _rows(self, first=0, count=None):
+        """Local rows of rows (2D) or planes (3D) first .. first + count - 1."""
+        count = self.count - first if count is None else count
+        per = self.ly if self.ndim == 3 else 1
+        return np.arange(first * per, (first + count) * per)
+
+    def _field(self, colour, r=None):
+        """Sum of the opposite colour's neighbours of the owned sites of `colour` in rows r."""
+        h, ly = self.halo, self.ly
         oth = self.a[1 - colour].astype(np.int64)
-        r = np.arange(rows)
+        r = np.arange(self.rows) if r is None else r
         z, y = (r // ly, r % ly) if self.ndim == 3 else (np.zeros_like(r), r)
         same = oth[h + r]
         par = ((self.par0 + y + z + colour) & 1)[:, None]
@@ -134,26 +141,32 @@ class CpuSlab:
             field += oth[h + r + ly] + oth[h + r - ly]
         return field
 
-    def half_sweep(self, colour, t, slot=-1):
-        own = self.a[colour][self.halo:self.halo + self.rows]
-        field = self._field(colour)
-        q0, n = self.row0 * self.lh // 4, self.rows * self.lh // 4
+    def half_sweep(self, colour, t, slot=-1, first=0, count=None):
+        r = self._rows(first, count)
+        if len(r) == 0:
+            return
+        own = self.a[colour][self.halo + r]
+        field = self._field(colour, r)
+        q0, n = (self.row0 + r[0]) * self.lh // 4, len(r) * self.lh // 4
         u = oracle.philox_range(q0, n, t, colour, 0, self.k0, self.k1).reshape(own.shape)
         d = 2 * self.ndim
         if self.heat:
-            own[:] = np.where(u < self.table[(field + d) // 2], 1, -1)
+            new = np.where(u < self.table[(field + d) // 2], 1, -1).astype(np.int8)
         else:
             x = own * field
             flip = (x <= 0) | (u < self.table[(x + d) // 2])
-            own[:] = np.where(flip, -own, own)
+            new = np.where(flip, -own, own).astype(np.int8)
+        self.a[colour][self.halo + r] = new
         if slot >= 0:
-            self.series[slot] += self.observables()
+            self.series[slot] += self._observe(r)
+
+    def _observe(self, r):
+        s1 = self.a[1][self.halo + r].astype(np.int64)
+        m = int(s1.sum() + self.a[0][self.halo + r].astype(np.int64).sum())
+        return m, -int((s1 * self._field(1, r)).sum())
 
     def observables(self):
-        h, r = self.halo, self.rows
-        s1 = self.a[1][h:h + r].astype(np.int64)
-        m = int(s1.sum() + self.a[0][h:h + r].astype(np.int64).sum())
-        return m, -int((s1 * self._field(1)).sum())
+        return self._observe(np.arange(self.rows))
 
     def series_reset(self, pairs):
         self.series = np.zeros((pairs, 2), np.int64)
@@ -184,11 +197,12 @@ def _assemble(shape, slabs):
     return oracle.from_compressed(c0, c1, shape)
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("shape,beta,algorithm,seed,parts", CASES)
-def test_local_exchange_matches_whole_lattice(shape, beta, algorithm, seed, parts):
+def test_local_exchange_matches_whole_lattice(shape, beta, algorithm, seed, parts, overlap):
     lat, series, final, obs = _oracle_run(shape, beta, algorithm, seed, 6, 2)
     slabs = [CpuSlab(lat, b, c, beta, seed, algorithm) for b, c in partition(shape[0], parts)]
-    runner = SlabRunner(slabs, LocalExchange())
+    runner = SlabRunner(slabs, LocalExchange(), overlap=overlap)
     got = runner.sweep(6, 2)
     np.testing.assert_array_equal(got, series)
     np.testing.assert_array_equal(_assemble(shape, slabs), final)
@@ -207,12 +221,13 @@ def _ring_worker(rank, world, port, queue):
         for shape, beta, algorithm, seed, _ in CASES:
             lat = oracle.random_lattice(shape, seed)
             b, c = partition(shape[0], world)[rank]
-            slab = CpuSlab(lat, b, c, beta, seed, algorithm)
-            runner = SlabRunner([slab], RingExchange(None, device="cpu"))
-            series = runner.sweep(5, 1)
-            runner.sweep(2)
-            obs = runner.observables_int()
-            out.append((series, b, slab.compressed(), obs))
+            for overlap in (False, True):
+                slab = CpuSlab(lat, b, c, beta, seed, algorithm)
+                runner = SlabRunner([slab], RingExchange(None, device="cpu"), overlap=overlap)
+                series = runner.sweep(5, 1)
+                runner.sweep(2)
+                obs = runner.observables_int()
+                out.append((series, b, slab.compressed(), obs))
         queue.put((rank, out))
     finally:
         dist.destroy_process_group()
@@ -240,14 +255,16 @@ def test_ring_exchange_world2_gloo():
         sim = oracle.OracleInt8(shape, beta, seed=seed, algorithm=algorithm, init=lat)
         want_series = sim.sweep(5, measure_every=1)
         sim.sweep(2)
-        for rank in (0, 1):
-            series, _, _, obs = got[rank][k]
-            np.testing.assert_array_equal(series, want_series)
-            assert obs == sim.observables_int()
-        parts = sorted((got[r][k][1], got[r][k][2]) for r in (0, 1))
-        c0 = np.concatenate([p[1][0] for p in parts])
-        c1 = np.concatenate([p[1][1] for p in parts])
-        np.testing.assert_array_equal(oracle.from_compressed(c0, c1, shape), sim.get_lattice())
+        for kk in (2 * k, 2 * k + 1):  # without and with overlap
+            for rank in (0, 1):
+                series, _, _, obs = got[rank][kk]
+                np.testing.assert_array_equal(series, want_series)
+                assert obs == sim.observables_int()
+            parts = sorted(((got[r][kk][1], r), got[r][kk][2]) for r in (0, 1))
+            c0 = np.concatenate([p[1][0] for p in parts])
+            c1 = np.concatenate([p[1][1] for p in parts])
+            np.testing.assert_array_equal(oracle.from_compressed(c0, c1, shape),
+                                          sim.get_lattice())
 
 
 # ------------------------------------------------------------------------------ GPU ---------
@@ -262,9 +279,9 @@ GPU_CASES = [
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("exchange", ["peer", "copy"])
+@pytest.mark.parametrize("exchange,overlap", [("peer", False), ("copy", False), ("copy", True)])
 @pytest.mark.parametrize("variant,shape,algorithm,beta,parts", GPU_CASES)
-def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts, exchange):
+def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts, exchange, overlap):
     from pyising_b200.backend import B200Int8, B200MultiSpin
     from pyising_b200.slab import SlabSimulation
 
@@ -272,7 +289,8 @@ def test_gpu_slabs_match_one_handle(variant, shape, algorithm, beta, parts, exch
     one_cls = B200MultiSpin if variant == "msc" else B200Int8
     one = one_cls(shape, beta, seed=seed, algorithm=algorithm, init="hot")
     split = SlabSimulation(shape, beta, seed=seed, algorithm=algorithm, variant=variant,
-                           init="hot", parts=parts, devices=[0], exchange=exchange)
+                           init="hot", parts=parts, devices=[0], exchange=exchange,
+                           overlap=overlap)
     np.testing.assert_array_equal(split.get_lattice(), one.get_lattice())
     want = one.sweep_measured(12, 3)
     got = split.sweep_measured(12, 3)
