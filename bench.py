@@ -490,6 +490,32 @@ def run_served_stream(n_jobs: int) -> dict:
             "tuned_batch_knobs": tuned["config"]}
 
 
+def run_slabs(wl: str, parts: int = 2, sweeps: int = 200) -> dict:
+    """The workload's lattice cut into `parts` slabs on this GPU (neighbour rows read in place),
+    timed with CUDA events on the slabs' stream after a warm-up; shows the slab path's own cost
+    against the single-lattice kernels (on separate GPUs the slabs run concurrently)."""
+    import torch
+
+    from pyising_b200.slab import SlabSimulation
+
+    variant, shape, alg, beta, init, seed, _, _ = WORKLOADS[wl]
+    sim = SlabSimulation(shape, beta, seed=seed, algorithm=alg, variant=variant, init="philox",
+                         parts=parts, devices=[torch.cuda.current_device()])
+    st = sim.runner.streams[0]
+    sim.sweep(20)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    sim.sweep(sweeps)
+    b.record(st)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    sim.close()
+    n = int(np.prod(shape))
+    return {"workload": f"{DESCRIPTION[wl].split(',')[0]} as {parts} slabs on one GPU",
+            "parts": parts, "sweeps": sweeps, "flips_per_ns": round(n * sweeps / (ms * 1e6), 2),
+            "exchange": "neighbour edge rows read in place (no copies)"}
+
+
 def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
     import torch
 
@@ -553,6 +579,8 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
                              "description": DESCRIPTION[other],
                              "launch_knobs": t_other if t_other else "library defaults"}
         line["other_configs"] = extras
+    if args.extras and world == 1:
+        line["slab_decomposition"] = run_slabs(wl)
     if args.batch and world == 1:
         line["batched_ensemble"] = run_batched_ensemble()
     if args.serve_jobs > 0 and world == 1:
