@@ -29,8 +29,7 @@ from pathlib import Path
 
 import numpy as np
 
-from .physics import (BETA_C_3D, TC_2D, TC_3D, Summary, binder_scan, magnetization_2d,
-                      temperature_scan)
+from .physics import BETA_C_3D, TC_2D, TC_3D, binder_scan, temperature_scan
 
 # Sizes, temperatures and run lengths: QUICK as the reference's QUICK (3D Binder sizes 8 and 16:
 # int8 rows need Lx % 8 == 0), FULL with the reference's FULL sizes and temperature grids
