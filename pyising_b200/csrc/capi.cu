@@ -3,7 +3,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "capi_internal.h"
 
@@ -25,6 +28,77 @@ int fail(int code, const char* fmt, ...)
 int cuda_fail(cudaError_t e, const char* what)
 {
     return fail(ISING_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+// Device memory of simulation handles comes from one stream-ordered pool per device that keeps
+// up to kPoolKeep bytes of freed memory for reuse: creating and destroying many simulations
+// (a scan, a validation run, jobs one at a time) then maps no memory and synchronises nothing.
+constexpr unsigned long long kPoolKeep = 8ull << 30;
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64] = {};
+
+cudaError_t pool_alloc(int device, void** p, size_t bytes, cudaStream_t st)
+{
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+        if (!g_pool[device]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = device;
+            const cudaError_t e = cudaMemPoolCreate(&g_pool[device], &props);
+            if (e != cudaSuccess) return e;
+            unsigned long long keep = kPoolKeep;
+            cudaMemPoolSetAttribute(g_pool[device], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = g_pool[device];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+// Pinned host buffers of the measured series, by size class (powers of two from 4 KiB), kept
+// for reuse (at most kPinnedKept per class).
+constexpr size_t kPinnedKept = 8;
+static std::mutex g_pinned_mu;
+static std::map<size_t, std::vector<void*>> g_pinned;
+
+static size_t pinned_class(size_t bytes)
+{
+    size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
+cudaError_t host_pinned_get(void** p, size_t bytes)
+{
+    const size_t c = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        auto& v = g_pinned[c];
+        if (!v.empty()) {
+            *p = v.back();
+            v.pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaMallocHost(p, c);
+}
+
+void host_pinned_put(void* p, size_t bytes)
+{
+    if (!p) return;
+    const size_t c = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        auto& v = g_pinned[c];
+        if (v.size() < kPinnedKept) {
+            v.push_back(p);
+            return;
+        }
+    }
+    cudaFreeHost(p);
 }
 
 int device_sm_count(int device)
@@ -271,24 +345,28 @@ int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uin
     }
     h->stream = h->own_stream_handle;
     for (int c = 0; c < 2; ++c) {
-        e = cudaMalloc(&h->c[c], h->colour_bytes);
+        e = pool_alloc(device, &h->c[c], h->colour_bytes, h->stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
+            h->c[c] = nullptr;
             ising_destroy(h);
-            return fail(ISING_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", h->colour_bytes,
+            return fail(ISING_ERR_NOMEM, "allocation of %zu bytes failed: %s", h->colour_bytes,
                         cudaGetErrorString(e));
         }
     }
-    e = cudaMalloc(&h->d_acc, 8 * sizeof(unsigned long long));
+    e = pool_alloc(device, (void**)&h->d_acc, 8 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        h->d_acc = nullptr;
         ising_destroy(h);
-        return fail(ISING_ERR_NOMEM, "cudaMalloc of the accumulators failed");
+        return fail(ISING_ERR_NOMEM, "allocation of the accumulators failed");
     }
-    e = cudaMemset(h->d_acc, 0, 8 * sizeof(unsigned long long));
+    e = cudaMemsetAsync(h->d_acc, 0, 8 * sizeof(unsigned long long), h->stream);
+    // the arrays are usable from any stream once their allocation has completed
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         ising_destroy(h);
-        return cuda_fail(e, "cudaMemset of the accumulators");
+        return cuda_fail(e, "initialising the accumulators");
     }
     *out = h;
     return ISING_OK;
@@ -299,11 +377,14 @@ int ising_destroy(ising_sim* h)
     if (!h) return ISING_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    // pool memory goes back to the pool, stream-ordered on the handle's own stream
+    cudaStream_t fs = h->own_stream_handle;
     for (int c = 0; c < 2; ++c)
-        if (h->c[c]) cudaFree(h->c[c]);
-    if (h->d_acc) cudaFree(h->d_acc);
-    if (h->d_series) cudaFree(h->d_series);
-    if (h->h_series) cudaFreeHost(h->h_series);
+        if (h->c[c]) cudaFreeAsync(h->c[c], fs);
+    if (h->d_acc) cudaFreeAsync(h->d_acc, fs);
+    if (h->d_series) cudaFreeAsync(h->d_series, fs);
+    if (h->h_series) host_pinned_put(h->h_series, (size_t)h->series_cap * 2 * sizeof(long long));
+    if (fs) cudaStreamSynchronize(fs);
     clear_graphs(h);
     if (h->d_flags) cudaFree(h->d_flags);
     if (h->d_label) cudaFree(h->d_label);
@@ -371,7 +452,7 @@ int ising_set_lattice(ising_sim* h, const int8_t* full)
     const long long rpc = rows_per_chunk(h);
     const size_t row_bytes = (size_t)2 * h->lh;
     int8_t* stage = nullptr;
-    TRY_CUDA(cudaMallocAsync((void**)&stage, rpc * row_bytes, h->stream));
+    TRY_CUDA(pool_alloc(h->device, (void**)&stage, rpc * row_bytes, h->stream));
     int rc = ISING_OK;
     for (long long r0 = 0; r0 < h->rows && rc == ISING_OK; r0 += rpc) {
         const long long nr = (r0 + rpc > h->rows) ? h->rows - r0 : rpc;
@@ -406,7 +487,7 @@ int ising_get_lattice(ising_sim* h, int8_t* full)
     const long long rpc = rows_per_chunk(h);
     const size_t row_bytes = (size_t)2 * h->lh;
     int8_t* stage = nullptr;
-    TRY_CUDA(cudaMallocAsync((void**)&stage, rpc * row_bytes, h->stream));
+    TRY_CUDA(pool_alloc(h->device, (void**)&stage, rpc * row_bytes, h->stream));
     int rc = ISING_OK;
     for (long long r0 = 0; r0 < h->rows && rc == ISING_OK; r0 += rpc) {
         const long long nr = (r0 + rpc > h->rows) ? h->rows - r0 : rpc;
@@ -829,20 +910,25 @@ int ensure_series(ising_sim* h, int64_t pairs)
 {
     if (pairs <= h->series_cap) return ISING_OK;
     clear_graphs(h);  // captured measured chunks point into the old buffer
-    if (h->d_series) cudaFree(h->d_series);
-    if (h->h_series) cudaFreeHost(h->h_series);
+    if (h->d_series) cudaFreeAsync(h->d_series, h->stream);
+    if (h->h_series) {
+        cudaStreamSynchronize(h->stream);  // no copy into it is still in flight
+        host_pinned_put(h->h_series, (size_t)h->series_cap * 2 * sizeof(long long));
+    }
     h->d_series = nullptr;
     h->h_series = nullptr;
     h->series_cap = 0;
     const size_t bytes = (size_t)pairs * 2 * sizeof(long long);
-    cudaError_t e = cudaMalloc(&h->d_series, bytes);
+    cudaError_t e = pool_alloc(h->device, (void**)&h->d_series, bytes, h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return fail(ISING_ERR_NOMEM, "cudaMalloc of %zu series bytes failed", bytes);
+        h->d_series = nullptr;
+        return fail(ISING_ERR_NOMEM, "allocation of %zu series bytes failed", bytes);
     }
-    e = cudaMallocHost(&h->h_series, bytes);
+    e = host_pinned_get((void**)&h->h_series, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        h->h_series = nullptr;
         return fail(ISING_ERR_NOMEM, "cudaMallocHost of %zu bytes failed", bytes);
     }
     h->series_cap = pairs;
