@@ -314,21 +314,25 @@ __global__ void sw_bond_kernel(const ClusterArgs a)
 __global__ void sw_cross_kernel(const ClusterArgs a, const TileGeo g)
 {
     const int nbonds = 2 * a.ndim;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.S;
-         q += (long long)gridDim.x * blockDim.x) {
+    const u32 S = (u32)a.S, lh = (u32)a.lh, ly = (u32)a.ly;  // S < 2^31
+    for (u32 q = blockIdx.x * blockDim.x + threadIdx.x; q < S; q += gridDim.x * blockDim.x) {
         const unsigned mask = a.bonds[q];
         if (!mask) continue;
-        const long long row = q / a.lh;
-        const int j = (int)(q - row * a.lh);
-        const int y = (int)(row % a.ly), z = (int)(row / a.ly);
+        const u32 row = q / lh;
+        const int j = (int)(q - row * lh);
+        const int y = (int)(row % ly), z = (int)(row / ly);
         const int y0 = y / g.R * g.R, j0 = j / g.W * g.W;
+        const int y1 = y0 + g.R < (int)ly ? y0 + g.R : (int)ly;  // the tile, clipped
+        const int j1 = j0 + g.W < (int)lh ? j0 + g.W : (int)lh;
+        // in 2D only sites on a tile's border rows or columns have bonds that leave it
+        if (a.ndim == 2 && y > y0 && y < y1 - 1 && j > j0 && j < j1 - 1) continue;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             if (k >= nbonds) break;
             if (!((mask >> k) & 1u)) continue;
             int ny, nj, nz;
             bond_end(a, k, y, j, z, ny, nj, nz);
-            if (nz == z && ny >= y0 && ny < y0 + g.R && nj >= j0 && nj < j0 + g.W) continue;
+            if (nz == z && ny >= y0 && ny < y1 && nj >= j0 && nj < j1) continue;
             const long long m = ((long long)nz * a.ly + ny) * a.lh + nj;
             uf_union(a.label, (int)q, (int)(a.S + m), a.err);
         }
