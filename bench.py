@@ -573,9 +573,13 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
             d = run_device(other, 3, 3, 0, 1, local, None, t_other)
             d.pop("sim")
             v, _, _, _, _, _, sw, b = WORKLOADS[other]
+            # int8: one Philox block per 4 sites, so the integer-pipe ceiling is rate / 0.25
+            rng_ceiling_other = rng["philox_calls_per_ns"] / 0.25 if v == "int8" else None
             extras[other] = {"flips_per_ns": round(d["value"], 2),
                              "ms_per_step": round(d["ms_per_step"], 4),
                              "pct_hbm_roofline": round(100 * d["value"] * b / peaks["hbm_gbs"], 2),
+                             "pct_philox_roofline": (round(100 * d["value"] / rng_ceiling_other, 2)
+                                                     if rng_ceiling_other else None),
                              "description": DESCRIPTION[other],
                              "launch_knobs": t_other if t_other else "library defaults"}
         line["other_configs"] = extras
