@@ -24,6 +24,7 @@
 //      an ancestor); the tile order of sites is their global order, so the final root of a
 //      cluster is its smallest site whatever the tile size;
 //   2. every label is replaced by its root (a read-only walk: only thread i writes label[i]);
+//      in 2D the flips walk to the roots themselves instead;
 //   3. every cluster flips with probability 1/2: bit (root & 127) of
 //      Philox((root >> 7, t, kFlipTag, 0), key), the same for all its sites.
 // Site g = c * S + row * lh + j (S = rows * lh sites per colour, the logical compressed index).
@@ -348,12 +349,15 @@ __global__ void sw_flatten_kernel(int* label, long long n, int* err)
         label[i] = uf_root(label, (int)i, err);
 }
 
+// Step 3.  WALK: each site walks up to its root itself (read-only), with no flattening pass
+// before; otherwise the labels are flat already.
+template <bool WALK>
 __global__ void sw_flip_kernel(const ClusterArgs a)
 {
     const long long n = 2 * a.S;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n;
          g += (long long)gridDim.x * blockDim.x) {
-        const int root = a.label[g];
+        const int root = WALK ? uf_root(a.label, (int)g, a.err) : a.label[g];
         const u32x4 r = philox4x32_10((u32)root >> 7, a.t, kFlipTag, 0u, a.k0, a.k1);
         const u32 w = (root & 64) ? ((root & 32) ? r.w : r.z) : ((root & 32) ? r.y : r.x);
         if ((w >> (root & 31)) & 1u) {
@@ -442,8 +446,13 @@ static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip)
         sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
         sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);
     }
-    sw_flatten_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S, a.err);
-    if (flip) sw_flip_kernel<<<grid, 256, 0, h->stream>>>(a);
+    // 2D: the flips walk to the roots themselves (no flattening pass); 3D, where the trees of
+    // the tiles' roots are deeper (every z bond leaves its tile), measured faster flattened first
+    // (256^3: 1046 vs 1131 us per update; 1024^2: 79 vs 85 us the other way round)
+    const bool walk = flip && h->ndim == 2;
+    if (!walk) sw_flatten_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S, a.err);
+    if (walk) sw_flip_kernel<true><<<grid, 256, 0, h->stream>>>(a);
+    else if (flip) sw_flip_kernel<false><<<grid, 256, 0, h->stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "cluster update launch");
     return ISING_OK;
