@@ -562,3 +562,94 @@ class SlabSimulation:
             self.close()
         except Exception:  # noqa: BLE001 - interpreter shutdown
             pass
+
+
+def main(argv=None) -> int:
+    """Run one lattice over slabs and print one JSON line (rank 0):
+
+        python -m pyising_b200.slab --shape 16384 16384 --variant msc --sweeps 1000 --every 10
+        torchrun --nproc-per-node 8 -m pyising_b200.slab --shape 65536 65536 --variant msc
+
+    Under torchrun (WORLD_SIZE > 1) each rank holds one slab on its GPU (NCCL halos, exchange
+    overlapped with the rows that read no halo); otherwise ``--parts`` slabs share this
+    process's GPUs.  The sweeps are timed with CUDA events on every slab's stream, maximum over
+    ranks; the whole-lattice (M, E) series and flips/ns are printed.
+    """
+    import argparse
+    import json
+    import os
+
+    import torch
+
+    ap = argparse.ArgumentParser(prog="python -m pyising_b200.slab")
+    ap.add_argument("--shape", type=int, nargs="+", required=True)
+    ap.add_argument("--variant", choices=["int8", "msc"], default="int8")
+    ap.add_argument("--algorithm", choices=["metropolis", "heatbath"], default="metropolis")
+    ap.add_argument("--beta", type=float, default=None, help="default: the critical coupling")
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--init", choices=["hot", "cold", "philox"], default="philox")
+    ap.add_argument("--sweeps", type=int, default=200)
+    ap.add_argument("--every", type=int, default=0, help="measure (M, E) every n sweeps")
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--parts", type=int, default=None, help="slabs in this process")
+    args = ap.parse_args(argv)
+    from .lattice import BETA_C_2D
+
+    beta = args.beta if args.beta is not None else (BETA_C_2D if len(args.shape) == 2
+                                                     else 0.221654626)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    group = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        group = "default"
+    sim = SlabSimulation(args.shape, beta, seed=args.seed, algorithm=args.algorithm,
+                         variant=args.variant, init=args.init, parts=args.parts, group=group)
+    sim.sweep(args.warmup)
+    streams = sim.runner.streams
+    starts, ends = [], []
+    for st in streams:
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(st)
+        starts.append(ev)
+    series = sim.sweep_measured(args.sweeps, args.every) if args.every else sim.sweep(args.sweeps)
+    for st in streams:
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(st)
+        ends.append(ev)
+    for ev in ends:
+        ev.synchronize()
+    ms = max(a.elapsed_time(b) for a, b in zip(starts, ends))
+    if group is not None:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    m, e = sim.observables_int()
+    rank = int(os.environ.get("RANK", "0"))
+    if rank == 0:
+        n = int(np.prod(args.shape))
+        print(json.dumps({
+            "shape": args.shape, "variant": args.variant, "algorithm": args.algorithm,
+            "beta": beta, "slabs": world if group else len(sim.slabs), "ranks": world,
+            "sweeps": args.sweeps, "ms": round(ms, 3),
+            "flips_per_ns": round(n * args.sweeps / (ms * 1e6), 2), "final_M_E": [m, e],
+            "series": series.tolist() if series is not None else None}), flush=True)
+    sim.close()
+    if group is not None:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
