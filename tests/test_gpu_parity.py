@@ -333,3 +333,27 @@ def test_c2_full_size_properties(B, oracle_mod):
     w0, w1 = c.colour_arrays()
     np.testing.assert_array_equal(w0, ref.w[0])
     np.testing.assert_array_equal(w1, ref.w[1])
+
+
+@pytest.mark.parametrize("variant", ["int8", "msc"])
+def test_handles_reusing_pooled_memory_start_clean(B, variant):
+    """Handles take their arrays from a pool that keeps freed memory: a handle created on memory
+    another handle left (other spins, other measurements) gives exactly the results of the first
+    handle of that configuration."""
+    cls = B.B200Int8 if variant == "int8" else B.B200MultiSpin
+    shape = (256, 256)
+
+    def run(seed, every):
+        sim = cls(shape, 0.44, seed=seed, init="hot")
+        series = sim.sweep_measured(40, every)
+        out = (series, sim.get_lattice(), sim.observables_int())
+        del sim
+        return out
+
+    first = run(5, 4)
+    for other in range(3):  # dirty the pooled memory with other lattices and series
+        run(100 + other, 1 + other)
+    again = run(5, 4)
+    np.testing.assert_array_equal(first[0], again[0])
+    np.testing.assert_array_equal(first[1], again[1])
+    assert first[2] == again[2]
