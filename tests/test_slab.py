@@ -3,7 +3,7 @@
 CPU: the sweep loop (SlabRunner) and both halo exchanges run on CPU slabs whose half-sweep is
 a NumPy restatement of the reference update (src/pyising/backends/numpy_backend.py:26-44)
 working only on the slab's rows and halos: in one process (LocalExchange) and as gloo ranks of
-world size 2 (RingExchange, the code path NCCL runs on GPUs).  Spins and (M, E) series must be
+world size 2 and 3 (RingExchange, the code path NCCL runs on GPUs).  Spins and (M, E) series must be
 bit-identical to the oracle running the whole lattice.
 
 GPU: the C-ABI slab handles (ising_slab_*) split over several slabs on one GPU must be
@@ -239,14 +239,16 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def test_ring_exchange_world2_gloo():
+@pytest.mark.parametrize("world", [2, 3])
+def test_ring_exchange_gloo(world):
+    """World 2: both ring neighbours are the same rank; world 3: they differ."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_ring_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_ring_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
-    got = dict(q.get(timeout=180) for _ in range(2))
+    got = dict(q.get(timeout=240) for _ in range(world))
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -256,11 +258,11 @@ def test_ring_exchange_world2_gloo():
         want_series = sim.sweep(5, measure_every=1)
         sim.sweep(2)
         for kk in (2 * k, 2 * k + 1):  # without and with overlap
-            for rank in (0, 1):
+            for rank in range(world):
                 series, _, _, obs = got[rank][kk]
                 np.testing.assert_array_equal(series, want_series)
                 assert obs == sim.observables_int()
-            parts = sorted(((got[r][kk][1], r), got[r][kk][2]) for r in (0, 1))
+            parts = sorted(((got[r][kk][1], r), got[r][kk][2]) for r in range(world))
             c0 = np.concatenate([p[1][0] for p in parts])
             c1 = np.concatenate([p[1][1] for p in parts])
             np.testing.assert_array_equal(oracle.from_compressed(c0, c1, shape),
