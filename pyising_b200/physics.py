@@ -1,15 +1,18 @@
 """Physics checks of the sweep path, in FP64 on the host, driven through the batched kernel.
 
-The exact results follow pyising's src/pyising/exact.py and the estimators its
-src/pyising/observables.py, restated from the published formulas:
+The exact results and estimators are written from the published physics; they provide the
+quantities pyising checks with (values, not code, of src/pyising/exact.py:19-94 and
+src/pyising/observables.py:28-85):
 
-* :func:`magnetization_2d` — Onsager/Yang spontaneous magnetisation (exact.py:19-25);
-* :func:`energy_2d` — Onsager's energy per spin of the infinite square lattice (exact.py:28-38);
-* :func:`log_partition_torus`, :func:`energy_torus`, :func:`specific_heat_torus` — the exact
-  partition function of the finite periodic m x n lattice (Kaufman 1949; Ferdinand & Fisher
-  1969; exact.py:51-94);
-* :func:`binning_error`, :func:`binder`, :func:`jackknife_binder_error`, :func:`crossing`
-  (observables.py:31-85).
+* :func:`magnetization_2d` — Onsager/Yang spontaneous magnetisation;
+* :func:`energy_2d` — Onsager's energy per spin of the infinite square lattice;
+* :func:`log_partition_torus`, :func:`energy_torus`, :func:`specific_heat_torus` — Kaufman's
+  exact partition function of the finite periodic m x n lattice with its first and second
+  derivatives in K taken analytically (pyising differentiates ln Z numerically; the two agree
+  to the truncation error of its differences, and this one agrees with a full enumeration of
+  small tori to rounding);
+* :func:`binning_error`, :func:`binder`, :func:`jackknife_binder_error`, :func:`crossing` —
+  block-mean error, Binder cumulant, its blocked jackknife error, crossing of two curves.
 
 :func:`temperature_scan` runs a whole scan (every temperature, algorithm and variant) as ONE
 batched ensemble — each lattice bit-identical to running it alone — and summarises the exact
@@ -36,115 +39,214 @@ TC_3D = 1.0 / BETA_C_3D
 
 # ------------------------------------------------------------------ exact results --------
 def magnetization_2d(T):
-    """(1 - sinh(2/T)^-4)^(1/8) below T_c, 0 above."""
-    T = np.asarray(T, dtype=float)
-    s = np.sinh(2.0 / T)
-    with np.errstate(invalid="ignore", divide="ignore"):
-        inner = np.clip(1.0 - s ** -4.0, 0.0, None)
-    return np.where(T < TC_2D, inner ** 0.125, 0.0)
+    """Spontaneous magnetisation per spin of the infinite square lattice (Onsager 1949, proved
+    by Yang 1952): m = [1 - sinh(2K)^-4]^(1/8) for T < T_c, 0 above (K = 1/T, J = 1)."""
+    K = 1.0 / np.asarray(T, dtype=float)
+    ordered = K > BETA_C_2D
+    s4 = np.sinh(2.0 * np.where(ordered, K, BETA_C_2D)) ** 4
+    return np.where(ordered, np.maximum(1.0 - 1.0 / s4, 0.0) ** 0.125, 0.0)
 
 
 def energy_2d(T):
-    """u(K) = -coth 2K [1 + (2/pi)(2 tanh^2 2K - 1) K_1(k^2)], k = 2 sinh 2K / cosh^2 2K
-    (K_1 the complete elliptic integral of the first kind, parameter m = k^2)."""
+    """Energy per spin of the infinite square lattice (Onsager 1944):
+
+        u = -coth(2K) [1 + (2/pi) (2 tanh^2(2K) - 1) K(q)],   q = 2 sinh(2K) / cosh^2(2K),
+
+    with K(q) the complete elliptic integral of the first kind of modulus q (scipy's ``ellipk``
+    takes the parameter q^2).  At T_c, q = 1 and the prefactor 2 tanh^2 - 1 vanishes faster than
+    K(q) diverges, so the bracket is exactly 1 there (u = -sqrt 2)."""
     from scipy.special import ellipk
 
     K = 1.0 / np.asarray(T, dtype=float)
-    k = 2.0 * np.sinh(2.0 * K) / np.cosh(2.0 * K) ** 2
-    m = np.minimum(k * k, 1.0 - 1e-16)  # the logarithmic singularity sits at T_c
-    t2 = np.tanh(2.0 * K) ** 2
-    return -(1.0 / np.tanh(2.0 * K)) * (1.0 + (2.0 / np.pi) * (2.0 * t2 - 1.0) * ellipk(m))
+    c2, s2 = np.cosh(2.0 * K), np.sinh(2.0 * K)
+    q2 = (2.0 * s2 / (c2 * c2)) ** 2
+    regular = q2 < 1.0
+    elliptic = np.where(regular, ellipk(np.where(regular, q2, 0.0)), 0.0)
+    bracket = 1.0 + (2.0 / np.pi) * (2.0 * (s2 / c2) ** 2 - 1.0) * elliptic
+    return -(c2 / s2) * bracket
 
 
-def _log_2cosh(x):
-    a = np.abs(x)
-    return a + np.log1p(np.exp(-2.0 * a))
+def _lncosh2(x):
+    """ln(2 cosh x) without overflow."""
+    return np.logaddexp(x, -x)
 
 
-def _log_abs_2sinh(x):
+def _lnsinh2(x):
+    """ln|2 sinh x| without overflow (x != 0)."""
     a = np.abs(x)
     with np.errstate(divide="ignore"):
-        return a + np.log1p(-np.exp(-2.0 * a)), np.sign(x)
+        return a + np.log(-np.expm1(-2.0 * a))
+
+
+class _KaufmanTorus:
+    """ln Z of the m x n periodic square lattice and its first two derivatives in K, analytic.
+
+    Kaufman (1949), in the form of Ferdinand & Fisher (1969):
+
+        Z = 1/2 (2 sinh 2K)^(mn/2) (Z_1 + Z_2 + Z_3 + Z_4),
+        Z_1 = prod_{l odd} 2 cosh(m g_l / 2),   Z_2 = prod_{l odd} 2 sinh(m g_l / 2),
+        Z_3 = prod_{l even} 2 cosh(m g_l / 2),  Z_4 = prod_{l even} 2 sinh(m g_l / 2),
+
+    l = 0 .. 2n-1, with cosh g_l = c(K) - cos(pi l / n), c(K) = sinh 2K + 1/sinh 2K, for l >= 1
+    and g_0 = 2K + ln tanh K, which changes sign at T_c (so Z_4 < 0 above T_c and Z_4 = 0 at
+    it).  Every factor but the one of g_0 is strictly positive (c >= 2), so each product is
+    kept as a log-magnitude plus its log-derivatives, and the g_0 factor of Z_4 is carried
+    separately: that keeps dZ_4/dK right at T_c, where Z_4 vanishes but its derivative does not.
+    The derivatives of g follow from cosh g = c(K): g' = c' / sinh g, g'' = (c'' - cosh g g'^2)
+    / sinh g.
+    """
+
+    def __init__(self, K: float, m: int, n: int):
+        self.K, self.m, self.n = float(K), int(m), int(n)
+        s = math.sinh(2.0 * K)
+        ch = math.cosh(2.0 * K)
+        l_odd = np.arange(1, 2 * n, 2, dtype=float)
+        l_even = np.arange(2, 2 * n, 2, dtype=float)  # l = 0 is handled on its own
+        c = s + 1.0 / s
+        dc = 2.0 * ch * (1.0 - 1.0 / (s * s))
+        ddc = 4.0 * s - 4.0 / s + 8.0 * ch * ch / s ** 3
+        half = 0.5 * self.m
+        self.x_odd = self._angles(l_odd, c, dc, ddc, half)
+        self.x_even = self._angles(l_even, c, dc, ddc, half)
+        g0 = 2.0 * K + math.log(math.tanh(K))
+        self.x0 = (half * g0, half * (2.0 + 2.0 / s), half * (-4.0 * ch / (s * s)))
+        self.lnpre = (0.5 * m * n) * math.log(2.0 * s)
+        self.dlnpre = m * n * ch / s
+        self.ddlnpre = -2.0 * m * n / (s * s)
+
+    def _angles(self, l, c, dc, ddc, half):
+        cg = c - np.cos(np.pi * l / self.n)
+        g = np.arccosh(cg)
+        sg = np.sqrt((cg - 1.0) * (cg + 1.0))
+        dg = dc / sg
+        ddg = (ddc - cg * dg * dg) / sg
+        return half * g, half * dg, half * ddg
+
+    @staticmethod
+    def _cosh_product(x, dx, ddx):
+        """(ln prod 2cosh x, its K-derivative, its second K-derivative)."""
+        t = np.tanh(x)
+        return (float(np.sum(_lncosh2(x))), float(np.sum(t * dx)),
+                float(np.sum((1.0 - t * t) * dx * dx + t * ddx)))
+
+    @staticmethod
+    def _sinh_product(x, dx, ddx):
+        """(ln prod 2sinh x, its K-derivative, its second K-derivative), every x > 0."""
+        ct = 1.0 / np.tanh(x)
+        return (float(np.sum(_lnsinh2(x))), float(np.sum(ct * dx)),
+                float(np.sum((1.0 - ct * ct) * dx * dx + ct * ddx)))
+
+    def derivatives(self) -> tuple[float, float, float]:
+        """(ln Z, d ln Z / dK, d^2 ln Z / dK^2)."""
+        x0, dx0, ddx0 = self.x0
+        # each term: (log-magnitude, value, first, second derivative) / exp(log-magnitude)
+        terms = []
+        for lnz, d1, d2 in (self._cosh_product(*self.x_odd), self._sinh_product(*self.x_odd)):
+            terms.append((lnz, 1.0, d1, d2 + d1 * d1))
+        # Z_3: the g_0 factor 2 cosh x0 is regular, fold it in
+        lnz, d1, d2 = self._cosh_product(*self.x_even)
+        t0 = math.tanh(x0)
+        d1 += t0 * dx0
+        d2 += (1.0 - t0 * t0) * dx0 * dx0 + t0 * ddx0
+        terms.append((lnz + float(_lncosh2(x0)), 1.0, d1, d2 + d1 * d1))
+        # Z_4 = f0 * R, f0 = 2 sinh x0 (may vanish), R = the remaining product
+        lnr, r1, r2 = self._sinh_product(*self.x_even)
+        f0 = 2.0 * math.sinh(x0)
+        f1 = 2.0 * math.cosh(x0) * dx0
+        f2 = f0 * dx0 * dx0 + 2.0 * math.cosh(x0) * ddx0
+        terms.append((lnr, f0, f1 + f0 * r1, f2 + 2.0 * f1 * r1 + f0 * (r2 + r1 * r1)))
+        top = max(t[0] for t in terms)
+        w = [math.exp(t[0] - top) for t in terms]
+        s0 = sum(wi * t[1] for wi, t in zip(w, terms))
+        s1 = sum(wi * t[2] for wi, t in zip(w, terms))
+        s2 = sum(wi * t[3] for wi, t in zip(w, terms))
+        lnz = -math.log(2.0) + self.lnpre + top + math.log(s0)
+        d1 = self.dlnpre + s1 / s0
+        d2 = self.ddlnpre + s2 / s0 - (s1 / s0) ** 2
+        return lnz, d1, d2
 
 
 def log_partition_torus(K: float, m: int, n: int) -> float:
-    """ln Z of the m x n periodic square lattice at coupling K.
-
-    Z = (1/2) (2 sinh 2K)^(mn/2) (Z_1 + Z_2 + Z_3 + Z_4), with Z_1 = prod_r 2 cosh(m g_{2r+1}/2),
-    Z_2 = prod_r 2 sinh(m g_{2r+1}/2), Z_3, Z_4 the same over g_{2r} (r = 0 .. n-1), where
-    cosh g_l = cosh 2K coth 2K - cos(pi l / n) and g_0 = 2K + ln tanh K (negative above T_c, so
-    Z_4 changes sign there).  Summed in log space with signs.
-    """
-    r = np.arange(n)
-    c = math.cosh(2.0 * K) / math.tanh(2.0 * K)
-
-    def gam(l):
-        g = np.arccosh(np.maximum(c - np.cos(np.pi * l / n), 1.0))
-        return np.where(l == 0, 2.0 * K + math.log(math.tanh(K)), g)
-
-    parts = []
-    for g in (gam(2 * r + 1), gam(2 * r)):
-        parts.append((float(np.sum(_log_2cosh(m * g / 2.0))), 1.0))
-        ls, sg = _log_abs_2sinh(m * g / 2.0)
-        parts.append((float(np.sum(ls)), float(np.prod(sg))))
-    top = max(v for v, _ in parts)
-    s = sum(sg * math.exp(v - top) for v, sg in parts if np.isfinite(v))
-    return (-math.log(2.0) + 0.5 * m * n * math.log(2.0 * math.sinh(2.0 * K)) + top
-            + math.log(s))
+    """ln Z of the m x n periodic square lattice at coupling K (J = 1, h = 0)."""
+    return _KaufmanTorus(K, m, n).derivatives()[0]
 
 
-def energy_torus(T: float, L: int, h: float = 1e-5) -> float:
-    """Exact energy per spin of the L x L torus: -(d ln Z / dK) / L^2 (central difference)."""
+def energy_torus(T: float, L: int) -> float:
+    """Exact energy per spin of the L x L torus, u = -(1/L^2) d ln Z / dK."""
+    return -_KaufmanTorus(1.0 / T, L, L).derivatives()[1] / (L * L)
+
+
+def specific_heat_torus(T: float, L: int) -> float:
+    """Exact specific heat per spin of the L x L torus, c = (K^2 / L^2) d^2 ln Z / dK^2."""
     K = 1.0 / T
-    return -(log_partition_torus(K + h, L, L) - log_partition_torus(K - h, L, L)) / (2 * h) / L**2
-
-
-def specific_heat_torus(T: float, L: int, h: float = 1e-4) -> float:
-    """Exact specific heat per spin of the L x L torus: K^2 (d^2 ln Z / dK^2) / L^2."""
-    K = 1.0 / T
-    f = [log_partition_torus(K + s * h, L, L) for s in (-1, 0, 1)]
-    return K * K * (f[0] - 2.0 * f[1] + f[2]) / (h * h) / L**2
+    return K * K * _KaufmanTorus(K, L, L).derivatives()[2] / (L * L)
 
 
 # ------------------------------------------------------------------ estimators -----------
-def binning_error(x, n_bins: int = 32) -> float:
-    """Standard error of the mean from n_bins equal blocks."""
+def _blocks(x, n_bins: int) -> np.ndarray | None:
+    """The series cut into ``min(n_bins, len)`` equal consecutive blocks (the tail that does not
+    fill a block is dropped), one row per block; None when fewer than two blocks exist."""
     x = np.asarray(x, dtype=float)
-    nb = min(n_bins, x.size)
+    nb = min(int(n_bins), x.size)
     if nb < 2:
+        return None
+    size = x.size // nb
+    return x[: nb * size].reshape(nb, size)
+
+
+def binning_error(x, n_bins: int = 32) -> float:
+    """Standard error of the mean of a correlated series, from the scatter of block means
+    (Flyvbjerg & Petersen 1989): blocks longer than the autocorrelation time are independent."""
+    b = _blocks(x, n_bins)
+    if b is None:
         return float("nan")
-    blocks = x[: x.size // nb * nb].reshape(nb, -1).mean(axis=1)
-    return float(blocks.std(ddof=1) / math.sqrt(nb))
+    means = b.mean(axis=1)
+    nb = means.size
+    var = float(np.sum((means - means.mean()) ** 2)) / (nb - 1)
+    return math.sqrt(var / nb)
+
+
+def _binder_from_moments(m2: float, m4: float) -> float:
+    return 1.0 - m4 / (3.0 * m2 * m2)
 
 
 def binder(m) -> float:
-    """U_4 = 1 - <m^4> / (3 <m^2>^2)."""
-    m = np.asarray(m, dtype=float)
-    return float(1.0 - np.mean(m ** 4) / (3.0 * np.mean(m ** 2) ** 2))
+    """Binder's fourth-order cumulant U_4 = 1 - <m^4> / (3 <m^2>^2) (Binder 1981): 2/3 in the
+    ordered phase, 0 for a Gaussian order parameter."""
+    m2 = np.asarray(m, dtype=float) ** 2
+    return _binder_from_moments(float(m2.mean()), float((m2 * m2).mean()))
 
 
 def jackknife_binder_error(m, n_bins: int = 32) -> float:
-    """Blocked jackknife error of :func:`binder`."""
-    m = np.asarray(m, dtype=float)
-    nb = min(n_bins, m.size)
-    if nb < 2:
+    """Jackknife error of :func:`binder` over blocks: U_4 is recomputed with each block left
+    out, and sigma^2 = (n - 1)/n sum_j (U_j - mean U)^2 (Efron 1982)."""
+    b = _blocks(m, n_bins)
+    if b is None:
         return float("nan")
-    blocks = m[: m.size // nb * nb].reshape(nb, -1)
-    m2, m4 = (blocks ** 2).mean(axis=1), (blocks ** 4).mean(axis=1)
-    s2, s4 = m2.sum(), m4.sum()
-    jk = 1.0 - ((s4 - m4) / (nb - 1)) / (3.0 * ((s2 - m2) / (nb - 1)) ** 2)
-    return float(math.sqrt((nb - 1) * np.mean((jk - jk.mean()) ** 2)))
+    sq = b * b
+    block_m2, block_m4 = sq.mean(axis=1), (sq * sq).mean(axis=1)
+    nb = block_m2.size
+    tot2, tot4 = float(block_m2.sum()), float(block_m4.sum())
+    u = np.array([_binder_from_moments((tot2 - a) / (nb - 1), (tot4 - c) / (nb - 1))
+                  for a, c in zip(block_m2, block_m4)])
+    return math.sqrt((nb - 1) / nb * float(np.sum((u - u.mean()) ** 2)))
 
 
 def crossing(Ts, u_a, u_b) -> float:
-    """Temperature where two Binder curves cross (linear interpolation of their difference)."""
+    """First temperature at which two Binder curves meet: the first grid point where their
+    difference is zero, or the zero of the straight line through the first pair of neighbours
+    with opposite signs; NaN when they do not cross on the grid."""
+    T = np.asarray(Ts, dtype=float)
     d = np.asarray(u_a, dtype=float) - np.asarray(u_b, dtype=float)
-    for i in range(len(d) - 1):
-        if d[i] == 0:
-            return float(Ts[i])
-        if d[i] * d[i + 1] < 0:
-            return float(Ts[i] - d[i] * (Ts[i + 1] - Ts[i]) / (d[i + 1] - d[i]))
-    return float("nan")
+    sign = np.sign(d)
+    hits = np.flatnonzero((sign[:-1] == 0) | (sign[:-1] * sign[1:] < 0))
+    if hits.size == 0:
+        return float("nan")
+    i = int(hits[0])
+    if d[i] == 0:
+        return float(T[i])
+    frac = d[i] / (d[i] - d[i + 1])
+    return float(T[i] + frac * (T[i + 1] - T[i]))
 
 
 @dataclass

@@ -18,15 +18,44 @@ from pyising_b200 import physics as ph
 
 
 def test_exact_results_match_the_reference():
+    """pyising takes the torus energy and specific heat as central differences of ln Z (steps
+    1e-5 and 1e-4); the values here are analytic derivatives, so they agree within the
+    truncation error of those differences (largest at L = 128 near T_c: ~6e-9 relative for
+    the energy, ~5e-5 absolute for the specific heat)."""
     g = golden("exact.npz")
     for i, T in enumerate(g["T"]):
         for j, L in enumerate(g["L"]):
             assert ph.energy_torus(float(T), int(L)) == pytest.approx(g["energy_torus"][i, j],
-                                                                       rel=1e-12)
+                                                                       rel=2e-8)
             assert ph.specific_heat_torus(float(T), int(L)) == pytest.approx(
-                g["specific_heat_torus"][i, j], rel=1e-9, abs=1e-9)
+                g["specific_heat_torus"][i, j], rel=1e-4, abs=1e-6)
     np.testing.assert_allclose(ph.magnetization_2d(g["T"]), g["magnetization_2d"], rtol=1e-13)
     np.testing.assert_allclose(ph.energy_2d(g["T"]), g["energy_2d"], rtol=1e-13)
+
+
+def _enumerated_torus(K: float, m: int, n: int) -> tuple[float, float, float]:
+    """ln Z, <sum of bonds> and its variance of the m x n torus by summing all 2^(mn) states."""
+    idx = np.arange(m * n).reshape(m, n)
+    right, down = np.roll(idx, -1, axis=1).ravel(), np.roll(idx, -1, axis=0).ravel()
+    states = ((np.arange(2 ** (m * n))[:, None] >> np.arange(m * n)) & 1) * 2 - 1
+    bonds = (states * states[:, right]).sum(1) + (states * states[:, down]).sum(1)
+    w = np.exp(K * (bonds - bonds.max()))
+    z = w.sum()
+    mean = float((w * bonds).sum() / z)
+    var = float((w * bonds * bonds).sum() / z) - mean * mean
+    return float(np.log(z)) + K * float(bonds.max()), mean, var
+
+
+@pytest.mark.parametrize("m,n", [(4, 4), (4, 5), (3, 6)])
+def test_kaufman_torus_equals_full_enumeration(m, n):
+    """ln Z and its first two K-derivatives equal the sums over every state of small tori."""
+    for K in (0.2, 0.35, ph.BETA_C_2D, 0.6, 1.0):
+        lnz, mean, var = _enumerated_torus(K, m, n)
+        assert ph.log_partition_torus(K, m, n) == pytest.approx(lnz, rel=1e-13)
+        if m == n:
+            assert ph.energy_torus(1.0 / K, m) == pytest.approx(-mean / (m * n), rel=1e-12)
+            assert ph.specific_heat_torus(1.0 / K, m) == pytest.approx(K * K * var / (m * n),
+                                                                        rel=1e-10)
 
 
 def test_torus_energy_tends_to_onsager_away_from_tc():
