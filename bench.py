@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload msc16384|int8_1024|int8_3d_256] [--no-extras]
+    python bench.py --profile-case CASE L SWEEPS   (one small case for ncu; no JSON line)
 
 Headline workload (one "step" = one whole job of the config): 2D multi-spin-coded Metropolis,
 L = 16384 (64 spins per uint64, 16384 x 128 words per colour), periodic, T = T_c, hot start
@@ -524,7 +525,7 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
     tuned = tune_workload(wl, local) if args.tune else None
     dev = run_device(wl, args.steps, args.warmup, rank, world, local, dist, tuned)
     sim = dev.pop("sim")
-    e2e = run_e2e(wl, max(1, min(args.steps, 3)), rank, world, dist, tuned)
+    e2e = run_e2e(wl, args.steps, rank, world, dist, tuned)
     if rank != 0:
         return None
     peaks = measured_peaks()
@@ -633,6 +634,71 @@ def main_reference(args, rank: int) -> dict | None:
                     "d2h_bytes_per_step": 0}}
 
 
+def profile_case(which: str, L: int, n: int) -> int:
+    """One small sweep case for profilers (ncu) and quick timing; prints the final exact (M, E)
+    (batch: of the first lattice) and no JSON line.
+
+    int8: 2D Metropolis L x L at beta_c, NumPy hot start seed 7; hb3: 3D heat bath L^3 at
+    beta = 0.221654626, cold start; msc: 2D multi-spin Metropolis L x L at beta_c, hot start
+    seed 7; sw: n Swendsen-Wang updates of a 2D int8 L x L lattice at beta_c from a cold start;
+    batch: an ensemble of 2D int8 Metropolis lattices L x L, L/2 x L/2 (four each) and L/4 x L/4
+    (sixteen) at temperatures 2.0 .. 2.6, device seeded starts, n sweeps with (M, E) every 10,
+    through the batched kernel; batch1: one 2D int8 Metropolis lattice L x L at beta_c alone in a
+    batch, device seeded start, no measurement; slab2 / mscslab2: a 2D int8 / msc Metropolis
+    L x L lattice at beta_c cut into two slabs on device 0 (neighbour rows read in place),
+    device seeded start."""
+    from pyising_b200.backend import B200Int8, B200MultiSpin
+    if which == "int8":
+        sim = B200Int8((L, L), BETA_C_2D, seed=7, init="hot")
+    elif which == "hb3":
+        sim = B200Int8((L, L, L), 0.221654626, seed=0, algorithm="heatbath", init="cold")
+    elif which == "msc":
+        sim = B200MultiSpin((L, L), BETA_C_2D, seed=7, init="hot")
+    elif which == "sw":
+        sim = B200Int8((L, L), BETA_C_2D, seed=7, init="cold")
+        sim.cluster_sweep(n)
+        sim.synchronize()
+        print(which, L, n, sim.observables_int())
+        return 0
+    elif which == "batch":
+        from pyising_b200.ensemble import Ensemble, Job
+
+        sizes = [L] + [L // 2] * 4 + [L // 4] * 16
+        jobs = [Job((s, s), 1.0 / (2.0 + 0.6 * i / len(sizes)), n, seed=i, measure_every=10,
+                    init="philox") for i, s in enumerate(sizes)]
+        with Ensemble() as ens:
+            ids = [ens.add(j) for j in jobs]
+            ens.run()
+            series = ens.result(ids[0]).series
+        print(which, L, n, tuple(int(x) for x in series[-1]) if len(series) else None)
+        return 0
+    elif which in ("slab2", "mscslab2"):
+        from pyising_b200.slab import SlabSimulation
+
+        sim = SlabSimulation((L, L), BETA_C_2D, seed=7, variant="msc" if which == "mscslab2"
+                             else "int8", init="philox", parts=2, devices=[0])
+        sim.sweep(n)
+        sim.synchronize()
+        print(which, L, n, sim.observables_int())
+        sim.close()
+        return 0
+    elif which == "batch1":
+        from pyising_b200.ensemble import Ensemble, Job
+
+        with Ensemble() as ens:
+            i = ens.add(Job((L, L), BETA_C_2D, n, seed=7, init="philox", keep_lattice=True))
+            ens.run()
+            lat = ens.result(i).lattice
+        print(which, L, n, int(lat.astype("int64").sum()))
+        return 0
+    else:
+        raise SystemExit(f"unknown case {which!r}")
+    sim.sweep(n)
+    sim.synchronize()
+    print(which, L, n, sim.observables_int())
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -651,7 +717,13 @@ def main() -> int:
                     help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--ref-step-s", type=float, default=2.0,
                     help="seconds of oracle work per step of --impl reference")
+    ap.add_argument("--profile-case", nargs=3, metavar=("CASE", "L", "SWEEPS"),
+                    help="run one small case for a profiler and exit (CASE: int8, hb3, msc, sw, "
+                         "batch, batch1, slab2, mscslab2)")
     args = ap.parse_args()
+    if args.profile_case:
+        which, L, n = args.profile_case
+        return profile_case(which, int(L), int(n))
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     rank, world, local = dist_env()

@@ -8,7 +8,7 @@
  *
  * The reference interface each entry point replaces is cited as file:line inside the pyising
  * project (github.com/walidhemati/pyising).  The Python host layer (pyising_b200.backend)
- * binds these through ctypes; INTEGRATION.md shows the binding a pyising maintainer adds.
+ * binds these through ctypes.
  */
 #ifndef ISING_B200_H
 #define ISING_B200_H
@@ -205,14 +205,19 @@ int ising_msc_calls_per_word(ising_sim* h, uint64_t t0, int64_t n_sweeps, double
 /* Sweeps on caller-owned device arrays that allocate nothing.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc (device memory owned by a pool they do not
  * control, or a loop that must not take cudaMalloc/cudaFree's implicit synchronisation).
- * c0, c1: the two colour arrays in device memory, laid out as ising_upload expects (int8
- * (rows, Lx/2) or packed uint64 (rows, Lx/128)), 16-byte aligned, updated in place.  Arguments
+ * c0, c1: the two colour arrays in device memory of the current device, laid out as
+ * ising_upload expects (int8 (rows, Lx/2): rows * Lx/2 bytes each, or packed uint64
+ * (rows, Lx/128): rows * Lx/16 bytes each), 16-byte aligned, updated in place.  Each must lie
+ * inside one device allocation with at least that many bytes from the pointer to the
+ * allocation's end; host memory, another GPU's memory or a shorter buffer is rejected with
+ * ISING_ERR_INVALID before any work is issued.  Arguments
  * otherwise as ising_create + ising_set_table + ising_sweep; the work runs on `stream`
  * (cudaStream_t, NULL = default stream) on the calling thread's current device.
  * Measured (M, E) sums live in a fixed 64 KiB device array inside the library (held by every
  * GPU that loads it until exit): at most 4096 measurements (n_sweeps / measure_every) per call,
  * more is rejected with ISING_ERR_INVALID.  The first call on a device looks the array's address
- * up (cudaGetSymbolAddress); make that first call before any stream capture.  Every call shares
+ * up (cudaGetSymbolAddress), and so does the first call after the device's context changed
+ * (cudaDeviceReset); make that first call before any stream capture.  Every call shares
  * the array, so calls that overlap on the GPU (other streams, other threads) race; the
  * measured part is cleared at the start of each call.  Blocks until series_out is written when
  * measure_every > 0, otherwise only enqueues the work. */

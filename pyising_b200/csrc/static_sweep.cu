@@ -10,8 +10,15 @@
 //
 // The scratch array is a file-scope __device__ symbol: every GPU that loads the library holds
 // its 64 KiB until the process exits.  Host code cannot use the symbol's name as an address
-// (on the host it names a host-side stand-in), so each device's real address is looked up once
-// with cudaGetSymbolAddress, with that device current, and cached.
+// (on the host it names a host-side stand-in), so each device's real address is looked up with
+// cudaGetSymbolAddress, with that device current, on the first call there, and cached with the
+// CUDA context it belongs to: after cudaDeviceReset the device has a new context, and the next
+// call looks the address up again.  The first call on a device does this set-up, so it should
+// come before any stream capture.
+//
+// Caller arrays are checked before any launch: they must be device (or managed) memory of the
+// current device, 16-byte aligned, and lie inside one allocation of at least the bytes the
+// shape needs (cuMemGetAddressRange through the runtime's driver entry points).
 #include <cstring>
 #include <mutex>
 
@@ -28,23 +35,49 @@ __device__ __align__(256) unsigned long long g_static_series[2 * kStaticSeriesMa
 constexpr int kMaxDevices = 64;
 std::mutex g_static_setup_mutex;
 unsigned long long* g_static_series_addr[kMaxDevices] = {};
+void* g_static_series_ctx[kMaxDevices] = {};
 
-// Device address of g_static_series on `device` (which must be current), looked up on the first
-// call for that device.
+// Driver entry points, looked up through the runtime (no link against libcuda).
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*MemGetAddressRangeFn)(unsigned long long* base, size_t* size,
+                                    unsigned long long ptr);
+
+template <typename Fn>
+Fn driver_entry(const char* name)
+{
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint(name, &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return reinterpret_cast<Fn>(fn);
+}
+
+// Device address of g_static_series on `device` (which must be current), looked up on the
+// first call for that device and again whenever the device's current context has changed.
 int static_series_address(int device, unsigned long long** out)
 {
     std::lock_guard<std::mutex> lock(g_static_setup_mutex);
-    if (!g_static_series_addr[device]) {
+    static CtxGetCurrentFn ctx_get = driver_entry<CtxGetCurrentFn>("cuCtxGetCurrent");
+    void* ctx = nullptr;
+    if (ctx_get && ctx_get(&ctx) != 0) ctx = nullptr;
+    if (!g_static_series_addr[device] || ctx != g_static_series_ctx[device]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_series);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static series scratch)");
         g_static_series_addr[device] = static_cast<unsigned long long*>(p);
+        g_static_series_ctx[device] = ctx;
     }
     *out = g_static_series_addr[device];
     return ISING_OK;
 }
 
-int check_device_array(const void* p, const char* name)
+// A caller array of at least `need` bytes on `device`: checked on the host before any launch,
+// so that a pointer to host memory, to another GPU or to a too-short buffer is an
+// ISING_ERR_INVALID and not a kernel reading out of bounds.
+int check_device_array(const void* p, const char* name, int device, size_t need)
 {
     if (!p) return fail(ISING_ERR_INVALID, "%s is null", name);
     if (reinterpret_cast<uintptr_t>(p) % 16)
@@ -57,6 +90,20 @@ int check_device_array(const void* p, const char* name)
     }
     if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
         return fail(ISING_ERR_INVALID, "%s must be device memory", name);
+    if (a.type == cudaMemoryTypeDevice && a.device != device)
+        return fail(ISING_ERR_INVALID, "%s lives on device %d, but device %d is current", name,
+                    a.device, device);
+    static MemGetAddressRangeFn range = driver_entry<MemGetAddressRangeFn>("cuMemGetAddressRange");
+    if (!range) return fail(ISING_ERR_CUDA, "cuMemGetAddressRange is not available");
+    unsigned long long base = 0;
+    size_t size = 0;
+    const unsigned long long ptr = reinterpret_cast<uintptr_t>(p);
+    if (range(&base, &size, ptr) != 0)
+        return fail(ISING_ERR_INVALID, "%s is not inside a device allocation", name);
+    if (ptr < base || ptr - base > size || size - (ptr - base) < need)
+        return fail(ISING_ERR_INVALID,
+                    "%s holds %llu bytes to the end of its allocation; the shape needs %llu",
+                    name, (unsigned long long)(size - (ptr - base)), (unsigned long long)need);
     return ISING_OK;
 }
 
@@ -101,15 +148,18 @@ extern "C" int ising_sweep_static(int ndim, const int64_t* shape, int variant, i
                     (long long)kStaticSeriesMaxPairs, (long long)n_meas);
     if (n_meas > 0 && !series_out)
         return fail(ISING_ERR_INVALID, "measure_every > 0 needs series_out");
-    int rc = check_device_array(c0, "c0");
-    if (rc == ISING_OK) rc = check_device_array(c1, "c1");
-    if (rc != ISING_OK) return rc;
-
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (device < 0 || device >= kMaxDevices)
         return fail(ISING_ERR_INVALID, "device ordinal %d not supported", device);
+    // bytes of one colour array: rows x Lx/2 int8, or rows x Lx/128 uint64 words
+    const size_t colour_bytes = variant == ISING_VARIANT_MSC
+                                    ? (size_t)rows * (size_t)(lx / 128) * sizeof(u64)
+                                    : (size_t)rows * (size_t)(lx / 2);
+    int rc = check_device_array(c0, "c0", device, colour_bytes);
+    if (rc == ISING_OK) rc = check_device_array(c1, "c1", device, colour_bytes);
+    if (rc != ISING_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int max_blocks = device_sm_count(device) * 8;
 

@@ -1,10 +1,10 @@
 """Generate the golden fixtures in this folder by running the pyising reference itself.
 
-Run once, in a checkout that has the reference source (the path below); the GPU host never runs
+Run once, with --reference pointing at the reference source; the GPU host never runs
 this.  Every array comes from the reference's own functions: ``pyising.philox``,
 ``pyising.lattice`` and the NumPy backends (``src/pyising/backends/numpy_backend.py``).
 
-    python tests/golden/make_golden.py [--reference /root/reference/src] [--quick]
+    python tests/golden/make_golden.py --reference <pyising checkout>/src [--quick]
 
 Files written (all ``.npz``):
   philox.npz      Philox4x32-10 known answers: the Random123 vectors listed in the reference's
@@ -86,7 +86,8 @@ def write_exact() -> None:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference/src")
+    ap.add_argument("--reference", required=True,
+                    help="the pyising source folder (the checkout's src/)")
     ap.add_argument("--quick", action="store_true", help="skip the long config runs")
     ap.add_argument("--only", choices=["exact"], default=None, help="write one fixture only")
     args = ap.parse_args()

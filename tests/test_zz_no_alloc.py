@@ -88,3 +88,71 @@ def test_static_sweep_rejects_more_measurements_than_the_scratch_holds():
                                   host.ctypes.data, d1.data_ptr(), 0, 1, 0, None, None)
     assert rc == 1
     assert "c0" in lib().ising_last_error().decode()
+
+
+def _cudart():
+    """The CUDA runtime torch already loaded (found by its soname), for exact-size allocations:
+    torch's caching allocator hands out pieces of larger segments."""
+    import torch
+
+    torch.cuda.init()
+    rt = ctypes.CDLL("libcudart.so.12")
+    rt.cudaMalloc.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t]
+    rt.cudaFree.argtypes = [ctypes.c_void_p]
+    return rt
+
+
+# shapes needing 4 MiB per colour, so the short arrays (2 MiB) stay short whatever granularity
+# the driver rounds allocations to
+@pytest.mark.parametrize("variant,shape", [("int8", (4096, 2048)), ("msc", (8192, 8192)),
+                                           ("int8", (64, 64, 2048))], ids=str)
+def test_static_sweep_rejects_arrays_shorter_than_the_shape(variant, shape):
+    """A colour array whose allocation ends before rows x (bytes per row) is refused before any
+    launch, naming the array; an allocation of exactly the needed size is accepted."""
+    from pyising_b200._lib import VARIANT, lib
+
+    rows = int(np.prod(shape[:-1]))
+    need = rows * shape[-1] // 2 if variant == "int8" else rows * shape[-1] // 128 * 8
+    rt = _cudart()
+    ptrs = []
+    try:
+        for size in (need, need // 2):
+            p = ctypes.c_void_p()
+            assert rt.cudaMalloc(ctypes.byref(p), size) == 0
+            ptrs.append(p.value)
+        full, short = ptrs
+        table = np.full(2 * len(shape) + 1, 0xFFFFFFFF, dtype=np.uint32)
+        for c0, c1, bad in ((short, full, "c0"), (full, short, "c1")):
+            rc = lib().ising_sweep_static(len(shape), _shape_arg(shape), VARIANT[variant], 0, 1,
+                                          table.ctypes.data, len(table), c0, c1, 0, 1, 0, None,
+                                          None)
+            assert rc == 1, bad  # ISING_ERR_INVALID
+            msg = lib().ising_last_error().decode()
+            assert msg.startswith(bad) and "needs" in msg, msg
+        # exactly the needed bytes (both arrays the same buffer: zero sweeps, nothing runs)
+        rc = lib().ising_sweep_static(len(shape), _shape_arg(shape), VARIANT[variant], 0, 1,
+                                      table.ctypes.data, len(table), full, full, 0, 0, 0, None,
+                                      None)
+        assert rc == 0, lib().ising_last_error().decode()
+    finally:
+        for p in ptrs:
+            rt.cudaFree(ctypes.c_void_p(p))
+
+
+def test_static_sweep_rejects_arrays_of_another_device():
+    """Arrays on a GPU other than the current one are refused before any launch."""
+    import torch
+
+    from pyising_b200._lib import lib
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    shape = (16, 32)
+    d0 = torch.ones(256, dtype=torch.int8, device="cuda:1")
+    d1 = torch.ones(256, dtype=torch.int8, device="cuda:1")
+    table = np.full(5, 0xFFFFFFFF, dtype=np.uint32)
+    with torch.cuda.device(0):
+        rc = lib().ising_sweep_static(2, _shape_arg(shape), 0, 0, 1, table.ctypes.data, 5,
+                                      d0.data_ptr(), d1.data_ptr(), 0, 1, 0, None, None)
+    assert rc == 1
+    assert "lives on device 1" in lib().ising_last_error().decode()
