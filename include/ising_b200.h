@@ -148,6 +148,11 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
  * 1 = no tiles: one union-find in global memory, else 32..6144); the labels are the same for
  * every value. */
 #define ISING_KNOB_CLUSTER_TILE 7
+/* Test hook of the bounded union-find loops (0 = off): 1 makes every cluster labeling write a
+ * two-site cycle into the labels (sites 0 and S) after the unions, so the root walks that follow
+ * run out of their step budgets and the call returns ISING_ERR_TIMEOUT, with the context intact.
+ * Never set outside tests. */
+#define ISING_KNOB_TEST_LABEL_CYCLE 8
 /* Batch and server knobs (ising_batch_set_knob, ising_server_set_knob): ISING_KNOB_BAND is the
  * longest band a kernel class may use (default 8); ISING_KNOB_ITEMS_PER_SLOT the work items per
  * resident block a launch aims at (default 6; smaller items balance better, larger ones cost

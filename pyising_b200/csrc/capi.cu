@@ -614,6 +614,10 @@ int ising_set_knob(ising_sim* h, int knob, int value)
                         "cluster tile must be 0 (automatic), 1 (no tiles) or 32..6144");
         h->cluster_tile = value;
         break;
+    case ISING_KNOB_TEST_LABEL_CYCLE:
+        if (value != 0 && value != 1) return fail(ISING_ERR_INVALID, "test hook is 0 or 1");
+        h->test_label_cycle = value;
+        break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
     clear_graphs(h);  // captured graphs hold the old launch parameters
@@ -631,6 +635,7 @@ int ising_get_knob(ising_sim* h, int knob, int* value)
     case ISING_KNOB_MSC_WAVES: *value = h->msc_waves; break;
     case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
     case ISING_KNOB_CLUSTER_TILE: *value = h->cluster_tile; break;
+    case ISING_KNOB_TEST_LABEL_CYCLE: *value = h->test_label_cycle; break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
     return ISING_OK;

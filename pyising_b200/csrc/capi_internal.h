@@ -53,6 +53,7 @@ struct ising_sim {
     unsigned int* d_flags = nullptr;    // persistent schedule: per-band progress + error word
     int* d_label = nullptr;             // cluster updates: a label per site, error word, masks
     int cluster_tile = 0;               // cluster updates: positions per tile (0: automatic)
+    int test_label_cycle = 0;           // test hook: a cycle in the cluster labels
     bool pending_err = false;           // a persistent run's error word not yet read
 };
 

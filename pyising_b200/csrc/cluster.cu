@@ -36,8 +36,36 @@ namespace ising {
 
 constexpr u32 kBondTag = 0x53570001u;  // Philox counter word 2 of the bond uniforms
 constexpr u32 kFlipTag = 0x53570002u;  // ... of the cluster flip bits
-constexpr long long kFindLimit = 1ll << 24;
-constexpr long long kUnionLimit = 1ll << 20;
+// Bounded loops: one union (its finds and retries) or one root walk may take at most kStepLimit
+// steps (about 0.3 s of dependent L2 reads; legitimate walks are far shorter), and every loop
+// gives up as soon as any thread has set the error word, which it reads every kErrPoll steps.
+// A thread that runs out sets the error word, so one cycle in the labels (which a correct
+// union-find never makes) ends the whole launch within milliseconds and the host reports
+// ISING_ERR_TIMEOUT with the context intact.
+constexpr int kStepLimit = 1 << 20;
+constexpr int kErrPoll = 64;
+
+struct StepBudget {
+    int left = kStepLimit;
+    bool dead = false;
+};
+
+// One more step of a bounded loop; false (and the error word set) when the budget is spent or
+// another thread has set the error word.
+__device__ __forceinline__ bool step(StepBudget& b, int* err)
+{
+    if (b.dead) return false;
+    if (--b.left < 0) {
+        atomicExch(err, 1);
+        b.dead = true;
+        return false;
+    }
+    if ((b.left & (kErrPoll - 1)) == 0 && *(volatile int*)err) {
+        b.dead = true;
+        return false;
+    }
+    return true;
+}
 
 struct ClusterArgs {
     int8_t* c[2];
@@ -50,16 +78,15 @@ struct ClusterArgs {
     u32 t, k0, k1, p_bond;
 };
 
-__device__ __forceinline__ int uf_find(int* label, int x, int* err)
+__device__ __forceinline__ int uf_find(int* label, int x, int* err, StepBudget& b)
 {
-    for (long long it = 0; it < kFindLimit; ++it) {
+    while (step(b, err)) {
         const int p = __ldcg(label + x);
         if (p == x) return x;
         const int gp = __ldcg(label + p);
         if (gp != p) label[x] = gp;  // path halving
         x = gp;
     }
-    atomicExch(err, 1);
     return x;
 }
 
@@ -67,21 +94,22 @@ __device__ __forceinline__ int uf_find(int* label, int x, int* err)
 // (label[x] = grandparent) could overwrite the root another thread has just written to label[x].
 __device__ __forceinline__ int uf_root(const int* label, int x, int* err)
 {
-    for (long long it = 0; it < kFindLimit; ++it) {
+    StepBudget b;
+    while (step(b, err)) {
         const int p = __ldcg(label + x);
         if (p == x) return x;
         x = p;
     }
-    atomicExch(err, 1);
     return x;
 }
 
 __device__ __forceinline__ void uf_union(int* label, int a, int b, int* err)
 {
-    for (long long it = 0; it < kUnionLimit; ++it) {
-        a = uf_find(label, a, err);
-        b = uf_find(label, b, err);
-        if (a == b) return;
+    StepBudget budget;  // shared by the finds and the retries of this union
+    while (step(budget, err)) {
+        a = uf_find(label, a, err, budget);
+        b = uf_find(label, b, err, budget);
+        if (budget.dead || a == b) return;
         if (a > b) {
             const int t = a;
             a = b;
@@ -92,7 +120,14 @@ __device__ __forceinline__ void uf_union(int* label, int a, int b, int* err)
         if (old == b) return;
         b = old;
     }
-    atomicExch(err, 1);
+}
+
+// Test hook (ISING_KNOB_TEST_LABEL_CYCLE): a two-site cycle in the labels, which the root walks
+// after it can only leave through their step budgets.
+__global__ void sw_cycle_kernel(int* label, long long S)
+{
+    label[0] = (int)S;
+    label[S] = 0;
 }
 
 // Colour-1 positions of the 2d bonds of colour-0 site n (the order of the bond bits): the same
@@ -118,37 +153,37 @@ __device__ __forceinline__ int8_t colour1_spin(const ClusterArgs& a, long long m
     return a.c[1][mrow * a.pitch + (m - mrow * a.lh)];
 }
 
-// Shared-memory union-find of one tile (same rules as the global one).
-__device__ __forceinline__ int tile_find(volatile int* lab, int x, int* err)
+// Shared-memory union-find of one tile (same rules and bounds as the global one).
+__device__ __forceinline__ int tile_find(volatile int* lab, int x, int* err, StepBudget& b)
 {
-    for (int it = 0; it < (1 << 20); ++it) {
+    while (step(b, err)) {
         const int p = lab[x];
         if (p == x) return x;
         const int gp = lab[p];
         if (gp != p) lab[x] = gp;
         x = gp;
     }
-    atomicExch(err, 1);
     return x;
 }
 
 __device__ __forceinline__ int tile_root(const volatile int* lab, int x, int* err)
 {
-    for (int it = 0; it < (1 << 20); ++it) {
+    StepBudget b;
+    while (step(b, err)) {
         const int p = lab[x];
         if (p == x) return x;
         x = p;
     }
-    atomicExch(err, 1);
     return x;
 }
 
 __device__ __forceinline__ void tile_union(int* lab, int a, int b, int* err)
 {
-    for (int it = 0; it < (1 << 20); ++it) {
-        a = tile_find(lab, a, err);
-        b = tile_find(lab, b, err);
-        if (a == b) return;
+    StepBudget budget;
+    while (step(budget, err)) {
+        a = tile_find(lab, a, err, budget);
+        b = tile_find(lab, b, err, budget);
+        if (budget.dead || a == b) return;
         if (a > b) {
             const int t = a;
             a = b;
@@ -158,7 +193,6 @@ __device__ __forceinline__ void tile_union(int* lab, int a, int b, int* err)
         if (old == b) return;
         b = old;
     }
-    atomicExch(err, 1);
 }
 
 // Rectangular tiles: a tile is R rows x W positions of one plane (y in [y0, y0 + R), j in
@@ -260,7 +294,7 @@ __global__ void __launch_bounds__(256) sw_local_kernel(const ClusterArgs a, cons
                 changed = 1;
             }
         }
-        if (!__syncthreads_or(changed)) break;
+        if (!__syncthreads_or(changed && !*(volatile int*)a.err)) break;
     }
     for (int i = threadIdx.x; i < 2 * rn * wn; i += blockDim.x) {
         const int cc = i >= rn * wn;
@@ -446,6 +480,7 @@ static int cluster_step(ising_sim* h, u32 t, u64 seed, u32 p_bond, bool flip)
         sw_init_kernel<<<grid, 256, 0, h->stream>>>(a.label, 2 * a.S);
         sw_bond_kernel<<<grid, 256, 0, h->stream>>>(a);
     }
+    if (h->test_label_cycle) sw_cycle_kernel<<<1, 1, 0, h->stream>>>(a.label, a.S);
     // 2D: the flips walk to the roots themselves (no flattening pass); 3D, where the trees of
     // the tiles' roots are deeper (every z bond leaves its tile), measured faster flattened first
     // (256^3: 1046 vs 1131 us per update; 1024^2: 79 vs 85 us the other way round)

@@ -118,6 +118,36 @@ def test_cluster_tile_knob_range():
             set_cluster_tile(sim, bad)
 
 
+@pytest.mark.parametrize("shape,tile", [((64, 64), 0), ((64, 64), 1), ((8, 16, 32), 0)], ids=str)
+def test_bounded_union_find_loops_report_a_timeout(shape, tile):
+    """The test hook writes a two-site cycle into the labels after the unions: every root walk
+    that reaches it spends its step budget (or sees another thread's error) and returns, the
+    call reports ISING_ERR_TIMEOUT within a fraction of a second, and the context still works."""
+    import time
+
+    from pyising_b200._lib import DeviceTimeout, IsingError, check, lib
+    from pyising_b200.backend import B200Int8
+
+    sim = B200Int8(shape, 2.0, seed=5, init="cold")  # every bond active: one spanning cluster
+    set_cluster_tile(sim, tile)
+    check(lib().ising_set_knob(sim._h, 8, 1), "set_knob")  # ISING_KNOB_TEST_LABEL_CYCLE
+    t0 = time.perf_counter()
+    with pytest.raises(DeviceTimeout):
+        sim.cluster_sweep(2)
+    assert time.perf_counter() - t0 < 5.0
+    with pytest.raises(IsingError):
+        sim.cluster_labels()
+    # the context is usable: the same handle without the hook, and a fresh one, both work
+    check(lib().ising_set_knob(sim._h, 8, 0), "set_knob")
+    sim.set_lattice(np.ones(shape, np.int8))
+    sim.cluster_sweep(2)
+    fresh = B200Int8(shape, 2.0, seed=5, init="cold")
+    fresh.cluster_sweep(2)
+    np.testing.assert_array_equal(sim.get_lattice(), fresh.get_lattice())
+    fresh.sweep(3)
+    assert set(np.unique(fresh.get_lattice())) <= {-1, 1}
+
+
 def test_cluster_sweeps_are_deterministic_and_keep_the_lattice_valid():
     from pyising_b200.backend import B200Int8
 
