@@ -1,0 +1,104 @@
+"""The benched configurations at their full sizes against the oracle, word for word.
+
+The reference checks its backends by running the same seeded job on two implementations and
+comparing the spins exactly (tests/test_backends.py:22-51, src/pyising/validate.py:69-93).  The
+jobs here are the ones bench.py times, unchanged, through the product API (single-lattice
+handles, and the batched engine for the ensemble); the oracle runs the same jobs on every host
+thread.  All results are integers, so every comparison is exact.
+
+* msc 2D Metropolis 16384^2 at T_c, seed 7, hot start, 1000 sweeps (the headline): final colour
+  arrays and (M, E); plus the series every 100 sweeps.
+* int8 3D heat bath 256^3, beta 0.221654626, cold start, 2000 sweeps with (M, E) every 10: the
+  200-point series and the final lattice.
+* The 96-lattice ensemble (L = 2^k, k ~ U{6..12}, T ~ U[2.0, 2.6], seed = index, hot starts,
+  5000 sweeps, (M, E) every 10) through the batched engine: every member's series and final
+  lattice for the 51 members up to 512^2 over all 5000 sweeps; for the 45 larger members (whose
+  5000 sweeps would take the oracle many minutes) the series over the first 100 sweeps, from a
+  second batched run of the whole ensemble cut to 100 sweeps.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BETA_C_2D = 0.44068679350977147
+BETA_3D = 0.221654626
+
+
+def test_headline_msc_16384_1000_sweeps(oracle_mod):
+    from pyising_b200.backend import B200MultiSpin
+
+    shape = (16384, 16384)
+    sim = B200MultiSpin(shape, BETA_C_2D, seed=7, init="hot")
+    st = sim.state()
+    series = sim.sweep_measured(1000, 100)
+    ref = oracle_mod.OracleMultiSpin(shape, BETA_C_2D, seed=7, init="cold")
+    ref.w = [np.ascontiguousarray(st["c0"]), np.ascontiguousarray(st["c1"])]
+    ref_series = ref.sweep(1000, measure_every=100)
+    np.testing.assert_array_equal(series, ref_series)
+    w0, w1 = sim.colour_arrays()
+    np.testing.assert_array_equal(w0, ref.w[0])
+    np.testing.assert_array_equal(w1, ref.w[1])
+    assert sim.observables_int() == ref.observables_int()
+    # the unmeasured sweep loop (the bench step) gives the same lattice
+    plain = B200MultiSpin.from_state(st)
+    plain.sweep(1000)
+    p0, p1 = plain.colour_arrays()
+    np.testing.assert_array_equal(p0, ref.w[0])
+    np.testing.assert_array_equal(p1, ref.w[1])
+
+
+def test_int8_3d_256_heatbath_2000_sweeps(oracle_mod):
+    from pyising_b200.backend import B200Int8
+
+    shape = (256, 256, 256)
+    sim = B200Int8(shape, BETA_3D, seed=0, algorithm="heatbath", init="cold")
+    series = sim.sweep_measured(2000, 10)
+    ref = oracle_mod.OracleInt8(shape, BETA_3D, seed=0, algorithm="heatbath", init="cold")
+    ref_series = ref.sweep(2000, measure_every=10)
+    assert series.shape == (200, 2)
+    np.testing.assert_array_equal(series, ref_series)
+    c0, c1 = sim.colour_arrays()
+    np.testing.assert_array_equal(c0, ref.c[0])
+    np.testing.assert_array_equal(c1, ref.c[1])
+
+
+def _run_batched(jobs):
+    from pyising_b200.ensemble import Ensemble
+
+    with Ensemble() as ens:
+        ids = [ens.add(j) for j in jobs]
+        ens.run()
+        return [ens.result(i) for i in ids]
+
+
+def test_ensemble_of_96_lattices_against_the_oracle(oracle_mod):
+    import dataclasses
+
+    from bench import c4_jobs
+
+    jobs = [dataclasses.replace(j, keep_lattice=True) for j in c4_jobs()]
+    assert len(jobs) == 96
+    full = _run_batched(jobs)
+    short_jobs = [dataclasses.replace(j, sweeps=100) for j in jobs if j.shape[0] > 512]
+    short = iter(_run_batched(short_jobs))
+    checked_full = checked_short = 0
+    for job, res in zip(jobs, full, strict=True):
+        assert res.series.shape == (500, 2)
+        ref = oracle_mod.OracleInt8(job.shape, job.beta, seed=job.seed, init=job.init)
+        if job.shape[0] <= 512:
+            np.testing.assert_array_equal(res.series, ref.sweep(5000, measure_every=10))
+            np.testing.assert_array_equal(res.lattice, ref.get_lattice())
+            checked_full += 1
+        else:
+            s = next(short)
+            want = ref.sweep(100, measure_every=10)
+            np.testing.assert_array_equal(s.series, want)
+            # the first 100 sweeps of the full run are the same as the short run's
+            np.testing.assert_array_equal(res.series[:10], want)
+            np.testing.assert_array_equal(s.lattice, ref.get_lattice())
+            checked_short += 1
+    assert (checked_full, checked_short) == (51, 45)
