@@ -404,14 +404,36 @@ def sequential_plain(jobs) -> tuple[float, list]:
     return time.perf_counter() - t0, out
 
 
-def run_batched_ensemble() -> dict:
-    """C4: batched vs one at a time, every lattice's series compared."""
+def c4_oracle_check(jobs, results) -> dict:
+    """Every member's series and final lattice against the oracle (all host threads), after
+    the timed region: the checker, not a measured path."""
+    import oracle
+
+    oracle.set_threads(oracle.cpu_count())
+    t0 = time.perf_counter()
+    bad = []
+    for i, (job, res) in enumerate(zip(jobs, results, strict=True)):
+        ref = oracle.OracleInt8(job.shape, job.beta, seed=job.seed, init=job.init)
+        series = ref.sweep(job.sweeps, measure_every=job.measure_every)
+        if not (np.array_equal(series, res.series) and np.array_equal(ref.get_lattice(),
+                                                                      res.lattice)):
+            bad.append(i)
+    return {"identical": not bad, "members": len(jobs), "mismatched": bad,
+            "compared": "every (M, E) of the series and the final lattice",
+            "oracle_seconds": round(time.perf_counter() - t0, 1),
+            "oracle_threads": oracle.cpu_count()}
+
+
+def run_batched_ensemble(check_oracle: bool = True) -> dict:
+    """C4: batched vs one at a time, every lattice's series compared (and with the oracle)."""
     import torch
 
     from pyising_b200 import autotune
     from pyising_b200.ensemble import Ensemble
 
-    jobs = c4_jobs()
+    import dataclasses
+
+    jobs = [dataclasses.replace(j, keep_lattice=True) for j in c4_jobs()]
     flips = sum(j.n_spins * j.sweeps for j in jobs)
     tuned = autotune.tune_ensemble(jobs, sweeps=256)
     with Ensemble(memory_budget=120e9) as ens:
@@ -422,9 +444,11 @@ def run_batched_ensemble() -> dict:
         t0 = time.perf_counter()
         ens.run()
         t_batch = time.perf_counter() - t0
-        batched = [ens.result(i).series for i in ids]
+        results = [ens.result(i) for i in ids]
+        batched = [r.series for r in results]
     t_seq, seq = sequential_plain(jobs)
     same = all(np.array_equal(a, b) for a, b in zip(batched, seq, strict=True))
+    oracle_check = c4_oracle_check(jobs, results) if check_oracle else None
     return {"workload": "96 2D int8 Metropolis lattices, L=2^k k~U{6..12}, T~U[2.0,2.6], "
                         "seed=index, NumPy hot start, 5000 sweeps, (E,M) every 10; "
                         "draws from default_rng(0)",
@@ -432,27 +456,34 @@ def run_batched_ensemble() -> dict:
             "batched_flips_per_ns": round(flips / t_batch / 1e9, 2),
             "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
             "speedup": round(t_seq / t_batch, 3), "bit_identical": bool(same),
+            "oracle_identical": oracle_check["identical"] if oracle_check else None,
+            "oracle_check": oracle_check,
             "tuned_batch_knobs": tuned["config"],
-            "timed": "uploads of the start lattices, all sweeps, series back to the host"}
+            "timed": "uploads of the start lattices, all sweeps, series and final lattices "
+                     "back to the host"}
 
 
-def run_served_stream(n_jobs: int) -> dict:
-    """C5 (scaled to n_jobs): Poisson arrivals into the server; vs one at a time."""
+def run_served_stream(n_jobs: int, baseline_jobs: int | None = None) -> dict:
+    """C5: Poisson arrivals of ``n_jobs`` jobs into the server; the same jobs one at a time with
+    the plain kernels (all of them, or the first ``baseline_jobs`` as a seeded subset), and the
+    server's queue depth and memory use sampled every 50 ms."""
     import threading
 
-    from pyising_b200.ensemble import Server
-
     from pyising_b200 import autotune
+    from pyising_b200.ensemble import Server
 
     arrivals, jobs = c5_jobs(n_jobs)
     flips = sum(j.n_spins * j.sweeps for j in jobs)
     submit_t = [0.0] * n_jobs
     ids = [0] * n_jobs
     tuned = autotune.tune_ensemble(jobs[: min(n_jobs, 100)], sweeps=256)
-    with Server(memory_budget=120e9) as srv:
+    budget = int(120e9)
+    peaks = {"pending": 0, "active": 0, "used_bytes": 0}
+    with Server(memory_budget=budget) as srv:
         for name, v in tuned["config"].items():
             srv.set_knob(name, v)
         start = time.perf_counter()
+        done = threading.Event()
 
         def feeder():
             for i, job in enumerate(jobs):
@@ -462,33 +493,54 @@ def run_served_stream(n_jobs: int) -> dict:
                 submit_t[i] = time.perf_counter()
                 ids[i] = srv.submit(job)
 
-        th = threading.Thread(target=feeder)
+        def monitor():
+            while not done.wait(0.05):
+                st = srv.status()
+                for k in peaks:
+                    peaks[k] = max(peaks[k], int(st[k]))
+
+        th, mon = threading.Thread(target=feeder), threading.Thread(target=monitor)
         th.start()
+        mon.start()
         th.join()
         results = []
         for i in range(n_jobs):
             srv.wait(ids[i])
             results.append(srv.result(ids[i]))
             srv.release(ids[i])
+        done.set()
+        mon.join()
     lat = np.array([r.latency_s for r in results])
     end = max(submit_t[i] + lat[i] for i in range(n_jobs))
     served_s = end - submit_t[0]
-    t_seq, seq = sequential_plain(jobs)
-    same = all(np.array_equal(r.series, s) for r, s in zip(results, seq, strict=True))
+    nb = n_jobs if baseline_jobs is None else max(1, min(baseline_jobs, n_jobs))
+    base_flips = sum(j.n_spins * j.sweeps for j in jobs[:nb])
+    t_seq, seq = sequential_plain(jobs[:nb])
+    same = all(np.array_equal(r.series, s) for r, s in zip(results[:nb], seq, strict=True))
+    served_rate = flips / served_s / 1e9
+    offered_rate = flips / (arrivals[-1] * 1e9)
+    seq_rate = base_flips / t_seq / 1e9
     return {"workload": f"{n_jobs} jobs of the served-stream mix (Poisson 200 jobs/s; 70% 2D "
                         "L~logU[128,8192] int8|msc, 30% 3D L~logU[32,256] int8 heat bath; "
                         "T_c +-15%; sweeps~logU[100,10000]; (E,M) every 10; device seeded "
                         "start), seed 2026",
-            "jobs": n_jobs, "flips": flips, "offered_flips_per_ns": round(
-                flips / (arrivals[-1] * 1e9), 2),
-            "served_s": round(served_s, 3), "served_flips_per_ns": round(flips / served_s / 1e9, 2),
+            "jobs": n_jobs, "flips": flips, "offered_flips_per_ns": round(offered_rate, 2),
+            "arrival_window_s": round(float(arrivals[-1]), 3),
+            "served_s": round(served_s, 3), "served_flips_per_ns": round(served_rate, 2),
+            "keeps_up": bool(served_rate >= 0.98 * offered_rate),
+            "sequential_jobs": nb,
+            "sequential_subset": ("all jobs" if nb == n_jobs else
+                                  f"the first {nb} jobs of the stream (seeded subset)"),
             "sequential_s": round(t_seq, 3),
-            "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
-            "speedup": round(t_seq / served_s, 3),
+            "sequential_flips_per_ns": round(seq_rate, 2),
+            "speedup": round(served_rate / seq_rate, 3),
             "latency_p50_s": round(float(np.percentile(lat, 50)), 4),
             "latency_p99_s": round(float(np.percentile(lat, 99)), 4),
-            "bit_identical": bool(same), "memory_budget_bytes": int(120e9),
-            "tuned_batch_knobs": tuned["config"]}
+            "latency_max_s": round(float(lat.max()), 4),
+            "peak_pending_jobs": peaks["pending"], "peak_active_jobs": peaks["active"],
+            "peak_used_bytes": peaks["used_bytes"],
+            "bit_identical": bool(same), "bit_identical_jobs": nb,
+            "memory_budget_bytes": budget, "tuned_batch_knobs": tuned["config"]}
 
 
 def run_slabs(wl: str, parts: int = 2, sweeps: int = 200) -> dict:
@@ -587,9 +639,9 @@ def main_b200(args, rank: int, world: int, local: int, dist) -> dict | None:
     if args.extras and world == 1:
         line["slab_decomposition"] = run_slabs(wl)
     if args.batch and world == 1:
-        line["batched_ensemble"] = run_batched_ensemble()
+        line["batched_ensemble"] = run_batched_ensemble(args.c4_oracle)
     if args.serve_jobs > 0 and world == 1:
-        line["served_stream"] = run_served_stream(args.serve_jobs)
+        line["served_stream"] = run_served_stream(args.serve_jobs, args.serve_baseline_jobs)
     torch.cuda.synchronize()
     return line
 
@@ -711,8 +763,12 @@ def main() -> int:
                     help="time the library's default launch knobs instead of tuned ones")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 96-lattice batched ensemble")
+    ap.add_argument("--no-c4-oracle", dest="c4_oracle", action="store_false",
+                    help="skip the oracle check of the 96 ensemble members (about 2 minutes)")
     ap.add_argument("--serve-jobs", type=int, default=300,
-                    help="jobs of the served stream (0 = skip)")
+                    help="jobs of the served stream (0 = skip; the configuration has 20000)")
+    ap.add_argument("--serve-baseline-jobs", type=int, default=None,
+                    help="time the one-at-a-time baseline on the first N jobs only")
     ap.add_argument("--cpu-budget", type=float, default=10.0,
                     help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--ref-step-s", type=float, default=2.0,

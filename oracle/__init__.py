@@ -52,6 +52,8 @@ def lib() -> ctypes.CDLL:
             "orc_msc_half": (I64, [P, P, P, I, U32, U64, U32, U32]),
             "orc_msc_observables": (None, [P, P, P, P, P]),
             "orc_msc_sweeps": (I64, [P, P, P, U64, I64, U64, U32, U32, I64, P]),
+            "orc_set_fast": (None, [I]),
+            "orc_fast_active": (I, []),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -63,6 +65,16 @@ def lib() -> ctypes.CDLL:
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+def set_fast(on: bool) -> None:
+    """int8 sweeps: the AVX-512 variant of the half-sweep where the host has it (default), or
+    the plain restatement; the two are bit-identical."""
+    lib().orc_set_fast(int(bool(on)))
+
+
+def fast_active() -> bool:
+    return bool(lib().orc_fast_active())
 
 
 def max_threads() -> int:

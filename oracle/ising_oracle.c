@@ -27,6 +27,8 @@
  *
  * Threads: the row loops are OpenMP-parallel (orc_set_threads); results do not depend on the
  * thread count because every site's random number is keyed by (site, sweep, colour, seed).
+ * The int8 sweeps use an AVX-512 variant of the half-sweep on hosts that have it (orc_set_fast;
+ * bit-identical to the plain one, both pinned to the golden vectors).
  */
 #include <math.h>
 #include <stdint.h>
@@ -171,6 +173,177 @@ void orc_int8_half(int8_t *own, const int8_t *other, int ndim, const int64_t *sh
     }
 }
 
+/* ---- the same half-sweep, vectorised with AVX-512 (x86-64 hosts that have it) -----------------
+ * Bit-identical to orc_int8_half (tests/test_oracle_golden.py checks both against each other
+ * and the golden vectors); it only makes the full-size parity runs affordable.  Per row: the
+ * row's Philox blocks sixteen at a time (32x32->64 products of even and odd lanes with
+ * vpmuludq), transposed into site order; then 64 sites per step: int8 neighbour sums, the
+ * table entry by a permute, an unsigned compare. */
+#if defined(__x86_64__) && defined(__GNUC__)
+#include <immintrin.h>
+#define ORC_AVX512 __attribute__((target("avx512f,avx512bw")))
+
+ORC_AVX512 static inline __m512i mulhi_lo(__m512i x, __m512i m, __m512i *lo)
+{
+    const __m512i pe = _mm512_mul_epu32(x, m);
+    const __m512i po = _mm512_mul_epu32(_mm512_srli_epi64(x, 32), m);
+    *lo = _mm512_mask_blend_epi32(0xAAAA, pe, _mm512_slli_epi64(po, 32));
+    return _mm512_mask_blend_epi32(0xAAAA, _mm512_srli_epi64(pe, 32), po);
+}
+
+/* Philox blocks (q0 + i, c1, c2, c3), i < 16, written in site order: out[4 i + w] = word w of
+ * block i. */
+ORC_AVX512 static void philox16(uint32_t q0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                uint32_t k1, uint32_t *out)
+{
+    __m512i x0 = _mm512_add_epi32(_mm512_set1_epi32((int)q0),
+                                  _mm512_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13,
+                                                    14, 15));
+    __m512i x1 = _mm512_set1_epi32((int)c1), x2 = _mm512_set1_epi32((int)c2);
+    __m512i x3 = _mm512_set1_epi32((int)c3);
+    const __m512i m0 = _mm512_set1_epi32((int)PHILOX_M0), m1 = _mm512_set1_epi32((int)PHILOX_M1);
+    for (int r = 0; r < 10; ++r) {
+        __m512i lo0, lo1;
+        const __m512i hi0 = mulhi_lo(x0, m0, &lo0);
+        const __m512i hi1 = mulhi_lo(x2, m1, &lo1);
+        const __m512i n0 = _mm512_ternarylogic_epi32(hi1, x1, _mm512_set1_epi32((int)k0), 0x96);
+        const __m512i n2 = _mm512_ternarylogic_epi32(hi0, x3, _mm512_set1_epi32((int)k1), 0x96);
+        x1 = lo1;
+        x3 = lo0;
+        x0 = n0;
+        x2 = n2;
+        k0 += PHILOX_W0;
+        k1 += PHILOX_W1;
+    }
+    /* 4 x 16 -> site order: 128-bit lane k of u_m holds block 4k + m after the unpacks */
+    const __m512i t0 = _mm512_unpacklo_epi32(x0, x1), t1 = _mm512_unpackhi_epi32(x0, x1);
+    const __m512i t2 = _mm512_unpacklo_epi32(x2, x3), t3 = _mm512_unpackhi_epi32(x2, x3);
+    const __m512i u0 = _mm512_unpacklo_epi64(t0, t2), u1 = _mm512_unpackhi_epi64(t0, t2);
+    const __m512i u2 = _mm512_unpacklo_epi64(t1, t3), u3 = _mm512_unpackhi_epi64(t1, t3);
+    const __m512i a = _mm512_shuffle_i32x4(u0, u1, 0x44), b = _mm512_shuffle_i32x4(u2, u3, 0x44);
+    const __m512i c = _mm512_shuffle_i32x4(u0, u1, 0xEE), d = _mm512_shuffle_i32x4(u2, u3, 0xEE);
+    _mm512_storeu_si512((void *)(out + 0), _mm512_shuffle_i32x4(a, b, 0x88));
+    _mm512_storeu_si512((void *)(out + 16), _mm512_shuffle_i32x4(a, b, 0xDD));
+    _mm512_storeu_si512((void *)(out + 32), _mm512_shuffle_i32x4(c, d, 0x88));
+    _mm512_storeu_si512((void *)(out + 48), _mm512_shuffle_i32x4(c, d, 0xDD));
+}
+
+/* 16 sites: flip / set mask from int8 values v (x = s h for Metropolis, h for heat bath). */
+ORC_AVX512 static inline __mmask16 decide16(__m128i v8, const uint32_t *u, __m512i tab,
+                                            int z2, int heatbath)
+{
+    const __m512i v = _mm512_cvtepi8_epi32(v8);
+    const __m512i idx = _mm512_srai_epi32(_mm512_add_epi32(v, _mm512_set1_epi32(z2)), 1);
+    const __m512i thr = _mm512_permutexvar_epi32(idx, tab);
+    const __mmask16 lt = _mm512_cmplt_epu32_mask(_mm512_loadu_si512((const void *)u), thr);
+    if (heatbath) return lt;
+    return lt | _mm512_cmple_epi32_mask(v, _mm512_setzero_si512());
+}
+
+ORC_AVX512 static void int8_half_avx512(int8_t *own, const int8_t *other, int ndim,
+                                        const int64_t *shape, int color, uint32_t t,
+                                        uint64_t seed, const uint32_t *table, int heatbath)
+{
+    const geom_t g = make_geom(ndim, shape);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const int z2 = 2 * ndim;
+    uint32_t tab16[16];
+    for (int i = 0; i < 16; ++i) tab16[i] = i <= z2 ? table[i] : 0u;
+    const __m512i tab = _mm512_loadu_si512((const void *)tab16);
+#pragma omp parallel
+    {
+        uint32_t *ubuf = (uint32_t *)malloc((size_t)(g.lh + 128) * sizeof(uint32_t));
+        int8_t *row = (int8_t *)malloc((size_t)g.lh + 2);
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < g.rows; ++r) {
+            const int64_t y = r % g.ly, zz = r / g.ly;
+            const int p = (int)((y + zz + color) & 1);
+            const int8_t *o = other + r * g.lh;
+            const int8_t *yu = other + (zz * g.ly + (y + 1 == g.ly ? 0 : y + 1)) * g.lh;
+            const int8_t *yd = other + (zz * g.ly + (y == 0 ? g.ly - 1 : y - 1)) * g.lh;
+            const int8_t *zu = other + ((zz + 1 == g.lz ? 0 : zz + 1) * g.ly + y) * g.lh;
+            const int8_t *zd = other + ((zz == 0 ? g.lz - 1 : zz - 1) * g.ly + y) * g.lh;
+            /* site uniforms of the row: ubuf[off + j] for site n = r lh + j */
+            const int64_t n0 = r * g.lh, q0 = n0 >> 2, q1 = (n0 + g.lh + 3) >> 2;
+            for (int64_t q = q0; q < q1; q += 16)
+                philox16((uint32_t)q, t, (uint32_t)color, 0u, k0, k1, ubuf + 4 * (q - q0));
+            const uint32_t *u = ubuf + (n0 & 3);
+            /* the row with its wrapped ends: row[1 + j] = o[j] */
+            row[0] = o[g.lh - 1];
+            memcpy(row + 1, o, (size_t)g.lh);
+            row[g.lh + 1] = o[0];
+            const int8_t *side = p ? row + 2 : row;
+            int8_t *s = own + r * g.lh;
+            for (int64_t j = 0; j < g.lh; j += 64) {
+                const int64_t left = g.lh - j;
+                const __mmask64 m = left >= 64 ? ~(__mmask64)0 : (((__mmask64)1 << left) - 1);
+                __m512i h = _mm512_add_epi8(_mm512_maskz_loadu_epi8(m, o + j),
+                                            _mm512_maskz_loadu_epi8(m, side + j));
+                h = _mm512_add_epi8(h, _mm512_maskz_loadu_epi8(m, yu + j));
+                h = _mm512_add_epi8(h, _mm512_maskz_loadu_epi8(m, yd + j));
+                if (ndim == 3) {
+                    h = _mm512_add_epi8(h, _mm512_maskz_loadu_epi8(m, zu + j));
+                    h = _mm512_add_epi8(h, _mm512_maskz_loadu_epi8(m, zd + j));
+                }
+                const __m512i sv = _mm512_maskz_loadu_epi8(m, s + j);
+                const __mmask64 neg = _mm512_movepi8_mask(sv);
+                /* Metropolis decides on x = s h, heat bath on h */
+                const __m512i v =
+                    heatbath ? h : _mm512_mask_sub_epi8(h, neg, _mm512_setzero_si512(), h);
+                __mmask64 f = 0;
+                for (int k = 0; k < 4; ++k)
+                    f |= (__mmask64)decide16(_mm512_extracti32x4_epi32(v, k), u + j + 16 * k, tab,
+                                             z2, heatbath)
+                         << (16 * k);
+                __m512i out;
+                if (heatbath) /* +1 where u < table, else -1 */
+                    out = _mm512_mask_blend_epi8(f, _mm512_set1_epi8(-1), _mm512_set1_epi8(1));
+                else
+                    out = _mm512_mask_sub_epi8(sv, f, _mm512_setzero_si512(), sv);
+                _mm512_mask_storeu_epi8(s + j, m, out);
+            }
+        }
+        free(ubuf);
+        free(row);
+    }
+}
+
+static int avx512_ok(void)
+{
+    static int ok = -1;
+    if (ok < 0) {
+        __builtin_cpu_init();
+        ok = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw");
+    }
+    return ok;
+}
+#else
+static int avx512_ok(void) { return 0; }
+static void int8_half_avx512(int8_t *own, const int8_t *other, int ndim, const int64_t *shape,
+                             int color, uint32_t t, uint64_t seed, const uint32_t *table,
+                             int heatbath)
+{
+    (void)own; (void)other; (void)ndim; (void)shape; (void)color; (void)t; (void)seed;
+    (void)table; (void)heatbath;
+}
+#endif
+
+/* 0 = the plain restatement above, 1 = the AVX-512 variant where the host has it (default). */
+static int g_fast = 1;
+
+void orc_set_fast(int on) { g_fast = on; }
+
+int orc_fast_active(void) { return g_fast && avx512_ok(); }
+
+static void int8_half(int8_t *own, const int8_t *other, int ndim, const int64_t *shape,
+                      int color, uint32_t t, uint64_t seed, const uint32_t *table, int heatbath)
+{
+    if (orc_fast_active())
+        int8_half_avx512(own, other, ndim, shape, color, t, seed, table, heatbath);
+    else
+        orc_int8_half(own, other, ndim, shape, color, t, seed, table, heatbath);
+}
+
 /* Integer observables of the int8 layout: M = sum of spins, E = -sum over bonds s_i s_j.
  * Every bond has exactly one colour-0 end (observables_torch.py:3-4). */
 void orc_int8_observables(const int8_t *c0, const int8_t *c1, int ndim, const int64_t *shape,
@@ -211,8 +384,8 @@ void orc_int8_sweeps(int8_t *c0, int8_t *c1, int ndim, const int64_t *shape, uin
     int64_t k = 0;
     for (int64_t s = 0; s < n; ++s) {
         const uint32_t t = (uint32_t)(t0 + (uint64_t)s);
-        orc_int8_half(c0, c1, ndim, shape, 0, t, seed, table, heatbath);
-        orc_int8_half(c1, c0, ndim, shape, 1, t, seed, table, heatbath);
+        int8_half(c0, c1, ndim, shape, 0, t, seed, table, heatbath);
+        int8_half(c1, c0, ndim, shape, 1, t, seed, table, heatbath);
         if (measure_every > 0 && (s + 1) % measure_every == 0 && series) {
             orc_int8_observables(c0, c1, ndim, shape, series + 2 * k, series + 2 * k + 1);
             ++k;

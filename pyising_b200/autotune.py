@@ -7,7 +7,10 @@ by site, sweep and colour, and every schedule visits the same sites with the sam
                     slide through its registers (the halo reuse depth); 0 = occupancy default;
 * ``chunk_width``   int8: bytes per thread and row, 16, 8 or 4 (4, 2 or 1 words of 4 sites);
 * ``blocks_per_sm`` grid size in blocks of 256 threads per SM;
-* ``msc_waves``     msc: contiguous warp ranges per resident warp of the work-stack kernel;
+* ``msc_kernel``    msc: schedule: word ranges per warp, or 32-word column strips walked down a
+                    band of rows with 4 or 3 Philox blocks per word at intake and registers
+                    bounded for 2, 3 or 4 resident blocks;
+* ``msc_waves``     msc: warps per resident warp (ranges or strip bands of the work-stack kernels);
 * ``graph_chunk``   sweeps per captured CUDA graph of an unmeasured run;
 * ``schedule``      ``"auto"`` (graphs), ``"launches"``, ``"persistent"`` or ``"temporal"``
                     (2D int8: two sweeps per launch on shared-memory tiles).
@@ -36,9 +39,10 @@ from pathlib import Path
 from . import _lib
 from ._lib import check, lib
 
-KNOBS = {"band": 1, "chunk_width": 2, "blocks_per_sm": 3, "msc_waves": 4, "graph_chunk": 5}
+KNOBS = {"band": 1, "chunk_width": 2, "blocks_per_sm": 3, "msc_waves": 4, "graph_chunk": 5,
+         "msc_kernel": 9}
 DEFAULTS = {"band": 0, "chunk_width": 16, "blocks_per_sm": 8, "msc_waves": 1, "graph_chunk": 32,
-            "schedule": "auto"}
+            "msc_kernel": 0, "schedule": "auto"}
 
 _lock = threading.Lock()
 _cache_mem: dict[Path, dict] = {}  # cache file contents by path, read once per process
@@ -75,6 +79,9 @@ def search_space(variant: str, shape, algorithm: str = "metropolis") -> dict[str
         space["band"] = [0, 1, 2, 4, 8, 16]
         space["chunk_width"] = [16, 4] + ([8] if lh % 8 == 0 else [])
     else:
+        # 0 = automatic; 1 = word ranges; 2..7 = column strips with (intake blocks, register
+        # bound) variants, where every row holds whole 32-word strips
+        space["msc_kernel"] = [0, 1] + ([2, 3, 4, 5, 6, 7] if (lh // 64) % 32 == 0 else [])
         space["msc_waves"] = [1, 2, 4]
     space["blocks_per_sm"] = [8, 4, 16]
     if variant == "int8" and len(shape) == 2:

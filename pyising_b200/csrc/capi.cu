@@ -614,6 +614,10 @@ int ising_set_knob(ising_sim* h, int knob, int value)
                         "cluster tile must be 0 (automatic), 1 (no tiles) or 32..6144");
         h->cluster_tile = value;
         break;
+    case ISING_KNOB_MSC_KERNEL:
+        if (value < 0 || value > 7) return fail(ISING_ERR_INVALID, "msc kernel must be 0..7");
+        h->msc_kernel = value;
+        break;
     case ISING_KNOB_TEST_LABEL_CYCLE:
         if (value != 0 && value != 1) return fail(ISING_ERR_INVALID, "test hook is 0 or 1");
         h->test_label_cycle = value;
@@ -635,6 +639,7 @@ int ising_get_knob(ising_sim* h, int knob, int* value)
     case ISING_KNOB_MSC_WAVES: *value = h->msc_waves; break;
     case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
     case ISING_KNOB_CLUSTER_TILE: *value = h->cluster_tile; break;
+    case ISING_KNOB_MSC_KERNEL: *value = h->msc_kernel; break;
     case ISING_KNOB_TEST_LABEL_CYCLE: *value = h->test_label_cycle; break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
@@ -961,7 +966,8 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         p.meas = meas;
         p.stats = stats;
         p.ctl = ctl;
-        e = launch_msc_half(true, p, h->max_blocks, h->sm_count, h->msc_waves, h->stream);
+        e = launch_msc_half(true, p, h->max_blocks, h->sm_count, h->msc_waves, h->stream,
+                            h->msc_kernel);
     } else {
         Int8Half p;
         p.own = (int8_t*)h->c[color];

@@ -39,6 +39,7 @@ struct ising_sim {
     // Launch knobs (ising_set_knob); every value gives identical results.
     int blocks_per_sm = 8;
     int msc_waves = 1;                  // msc: warp ranges per resident warp
+    int msc_kernel = 0;                 // msc: schedule (ISING_KNOB_MSC_KERNEL)
     int64_t graph_chunk = 32;           // sweeps per captured graph of an unmeasured run
     // Captured chunks of `sweeps` sweeps (one measurement at the end when `measured`), replayed
     // with the sweep counter and series slot in d_acc[6], d_acc[7].
@@ -83,8 +84,11 @@ int int8_default_band(long long rows, int ly, int cpr, int sm_count);
 unsigned int8_band_geometry(Int8Half& p, int max_blocks, int sm_count);
 cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_blocks, int sm_count,
                              cudaStream_t st);
+// kernel: 0 = automatic (the strip schedule where the rows hold whole 32-word strips), 1 = the
+// range schedule, 2..7 = the strip schedule with (Philox blocks per word at intake, resident
+// blocks the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4).
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int sm_count,
-                            int waves, cudaStream_t st);
+                            int waves, cudaStream_t st, int kernel = 0);
 cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,
                               long long row0, int lh, int pitch, int ly, int max_blocks,
                               cudaStream_t st);

@@ -322,6 +322,161 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Strip schedule (lattices whose rows hold a multiple of 32 words): a warp walks a band of rows
+// of one 32-word column strip, lane l owning word x0 + l of every row.  The opposite colour's
+// rows y - 1, y, y + 1 slide through registers (one new row per step), so a word costs three
+// loads (its own word, the opposite colour's next row, the horizontal neighbour word) instead
+// of five, and the row parity, the row index and the wrap of the vertical neighbours are
+// warp-uniform.  The bit-sliced count takes seven operations per 32-bit half: with
+// x_k = o ^ n_k, x1 ^ x2 = n1 ^ n2 and x1 & x2 = (o ^ n1) & (o ^ n2), so the pair sums need
+// no x_k.  The lazy comparison handles both levels of a Philox block together (seven
+// operations per half).  Words still undecided after the intake go to the warp's stack as in
+// the range schedule.  Random numbers, levels and their order are the reference's, so the
+// results are identical.
+
+// Pair sums of two anti-aligned flags: s = exactly one, c = both.
+struct HalfSlices {
+    u32 a1, a2;  // exactly one / two or more anti-aligned neighbours
+};
+
+__device__ __forceinline__ HalfSlices slice_half(u32 o, u32 n1, u32 n2, u32 n3, u32 n4)
+{
+    const u32 s1 = n1 ^ n2, c1 = (o ^ n1) & (o ^ n2);
+    const u32 s2 = n3 ^ n4, c2 = (o ^ n3) & (o ^ n4);
+    const u32 cc = c1 | c2;
+    HalfSlices h;
+    h.a1 = (s1 ^ s2) & ~cc;
+    h.a2 = cc | (s1 & s2);
+    return h;
+}
+
+// Both levels of one Philox block on 32 lanes: the even level uses r_e, the odd one r_o.
+__device__ __forceinline__ void level_pair(u32 re, u32 ro, u32 t4e, u32 t8e, u32 t4o, u32 t8o,
+                                           u32 a1, u32& und, u32& acc)
+{
+    const u32 tme = (a1 & t4e) | (~a1 & t8e);
+    const u32 tmo = (a1 & t4o) | (~a1 & t8o);
+    const u32 ae = und & ~re & tme;       // decided at the even level, accepted
+    const u32 u1 = und & ~(re ^ tme);     // still undecided after it
+    const u32 ao = u1 & ~ro & tmo;
+    und = u1 & ~(ro ^ tmo);
+    acc |= ae | ao;
+}
+
+__device__ __forceinline__ void block_levels(const u32x4& r, const uint4& m, u32 a1l, u32 a1h,
+                                             u32& undl, u32& undh, u32& accl, u32& acch)
+{
+    level_pair(r.x, r.z, m.x, m.y, m.z, m.w, a1l, undl, accl);  // r0 | r1 << 32, r2 | r3 << 32
+    level_pair(r.y, r.w, m.x, m.y, m.z, m.w, a1h, undh, acch);
+}
+
+// The warp updates rows [y0, y1) of strip `strip` (words 32 strip .. 32 strip + 31 of a row).
+template <int K>
+__device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int y0, int y1,
+                                               QueueSlots& q, const uint4* lvmask)
+{
+    const int lane = threadIdx.x & 31;
+    const u32 lt = (1u << lane) - 1u;
+    const int nw = p.nw, rows = p.rows;
+    const int x = strip * 32 + lane;
+    const int xr = x + 1 == nw ? 0 : x + 1, xl = x == 0 ? nw - 1 : x - 1;
+    const u64* other = p.other;
+    // opposite-colour rows y - 1 and y, then per step the next row, own word and side word
+    u64 up = __ldg(other + (long long)(y0 == 0 ? rows - 1 : y0 - 1) * nw + x);
+    u64 c = __ldg(other + (long long)y0 * nw + x);
+    u64 n_own = 0, n_dn = 0, n_side = 0;
+    auto fetch = [&](int y) {
+        const long long rb = (long long)y * nw;
+        n_own = p.own[rb + x];
+        n_dn = __ldg(other + (long long)(y + 1 == rows ? 0 : y + 1) * nw + x);
+        n_side = __ldg(other + rb + (((y + (int)p.color) & 1) ? xr : xl));
+    };
+    int y = y0;
+    if (y < y1) fetch(y);
+    int n = 0;
+    while (true) {
+        if (n < kPop && y < y1) {
+            const u64 o = n_own, dn = n_dn, side = n_side;
+            const bool odd = ((y + (int)p.color) & 1) != 0;
+            const u64 hz = odd ? ((c >> 1) | (side << 63)) : ((c << 1) | (side >> 63));
+            const int yc = y;
+            ++y;
+            if (y < y1) fetch(y);
+            const HalfSlices sl = slice_half((u32)o, (u32)c, (u32)hz, (u32)up, (u32)dn);
+            const HalfSlices sh = slice_half((u32)(o >> 32), (u32)(c >> 32), (u32)(hz >> 32),
+                                             (u32)(up >> 32), (u32)(dn >> 32));
+            up = c;
+            c = dn;
+            u32 undl = ~sl.a2, undh = ~sh.a2, accl = 0, acch = 0;
+            const u32 w = (u32)((long long)yc * nw + x);
+#pragma unroll
+            for (int b = 0; b < K; ++b) {
+                const u32x4 r = philox4x32_10(w, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
+                block_levels(r, level_masks(p.thr4, p.thr8, (u32)b), sl.a1, sh.a1, undl, undh,
+                             accl, acch);
+            }
+            const u32 resl = (u32)o ^ sl.a2 ^ accl, resh = (u32)(o >> 32) ^ sh.a2 ^ acch;
+            const bool keep = (undl | undh) != 0;
+            if (!keep) p.own[w] = (u64)resl | ((u64)resh << 32);
+            const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
+            if (keep) {
+                const int pos = n + __popc(km & lt);
+                q.idx[pos] = w;
+                q.lp[pos] = (u32)K;
+                q.a1[pos] = (u64)sl.a1 | ((u64)sh.a1 << 32);
+                q.und[pos] = (u64)undl | ((u64)undh << 32);
+                q.res[pos] = (u64)resl | ((u64)resh << 32);
+            }
+            n += __popc(km);
+            __syncwarp();
+        } else if (n > 0) {
+            // one Philox block for each of up to 32 entries at its own level pair; the result
+            // word of an entry already holds every decision made so far
+            const int take = n < 32 ? n : 32;
+            const int base = n - take;
+            const bool act = lane < take;
+            const int e = base + lane;
+            const u32 idx = act ? q.idx[e] : 0u;
+            u32 lp = act ? q.lp[e] : 0u;
+            const u64 a1 = act ? q.a1[e] : 0ull;
+            const u64 und = act ? q.und[e] : 0ull, res = act ? q.res[e] : 0ull;
+            __syncwarp();
+            u32 undl = (u32)und, undh = (u32)(und >> 32), accl = 0, acch = 0;
+            if (act) {
+                const u32x4 r = philox4x32_10(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
+                block_levels(r, lvmask[lp], (u32)a1, (u32)(a1 >> 32), undl, undh, accl, acch);
+                ++lp;
+            }
+            const u64 nres = res ^ ((u64)accl | ((u64)acch << 32));
+            const bool keep = act && (undl | undh) != 0 && lp < 16u;
+            if (act && !keep) p.own[idx] = nres;
+            const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
+            if (keep) {
+                const int pos = base + __popc(km & lt);
+                q.idx[pos] = idx;
+                q.lp[pos] = lp;
+                q.a1[pos] = a1;
+                q.und[pos] = (u64)undl | ((u64)undh << 32);
+                q.res[pos] = nres;
+            }
+            n = base + __popc(km);
+            __syncwarp();
+        } else {
+            break;
+        }
+    }
+}
+
+// (M, E) contributions of rows [y0, y1) of a strip after the warp updated them.
+__device__ __forceinline__ void msc_measure_strip(const MscHalf& p, int strip, int y0, int y1,
+                                                  long long& m_acc, long long& e_acc)
+{
+    long long calls = 0, wmax = 0;
+    const int x = strip * 32 + (threadIdx.x & 31);
+    for (int y = y0; y < y1; ++y) msc_word<false>(p, y, x, m_acc, e_acc, calls, wmax);
+}
+
 // (M, E) contributions of words [begin, end) as they are now, one word per lane of the warp:
 // run after the warp's msc_queue_range (and a __syncwarp) to measure the updated colour.
 __device__ __forceinline__ void msc_measure_range(const MscHalf& p, long long begin, long long end,

@@ -18,7 +18,8 @@ from pyising_b200 import autotune
 
 # ------------------------------------------------------------------------- CPU --------------
 @pytest.mark.parametrize("variant,shape", [("int8", (64, 64)), ("int8", (16, 16, 40)),
-                                           ("int8", (24, 1032)), ("msc", (128, 256))])
+                                           ("int8", (24, 1032)), ("msc", (128, 256)),
+                                           ("msc", (64, 4096))])
 def test_search_space_starts_at_the_defaults(variant, shape):
     space = autotune.search_space(variant, shape)
     for name, values in space.items():
@@ -31,6 +32,7 @@ def test_search_space_starts_at_the_defaults(variant, shape):
         assert "msc_waves" not in space
     else:
         assert "band" not in space and "chunk_width" not in space
+        assert (7 in space["msc_kernel"]) == (shape[-1] % 4096 == 0)
 
 
 def test_cache_round_trip(tmp_path):
@@ -56,6 +58,7 @@ CASES = [
     ("int8", (24, 48), "heatbath", 0.42),
     ("int8", (16, 16, 32), "heatbath", 0.22),
     ("msc", (128, 256), "metropolis", 0.44),
+    ("msc", (40, 4096), "metropolis", 0.44),  # 32-word rows: the strip schedules too
 ]
 
 

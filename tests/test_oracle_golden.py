@@ -70,8 +70,22 @@ def test_threshold_tables(oracle_mod):
         np.testing.assert_array_equal(threshold_table(beta, ndim, name), want)
 
 
+@pytest.fixture(params=["plain", "avx512"])
+def int8_path(request, oracle_mod):
+    """Both int8 half-sweeps of the oracle: the plain restatement and its AVX-512 variant (where
+    the host has AVX-512), each pinned to the same golden vectors."""
+    if request.param == "avx512":
+        oracle_mod.set_fast(True)
+        if not oracle_mod.fast_active():
+            pytest.skip("no AVX-512 on this host")
+    else:
+        oracle_mod.set_fast(False)
+    yield request.param
+    oracle_mod.set_fast(True)
+
+
 @pytest.mark.parametrize("case", int8_cases(), ids=lambda c: f"{c['shape']}-{c['algorithm']}")
-def test_int8_identity_cases(oracle_mod, case):
+def test_int8_identity_cases(oracle_mod, int8_path, case):
     lat = oracle_mod.random_lattice(case["shape"], case["init_seed"])
     sim = oracle_mod.OracleInt8(case["shape"], case["beta"], seed=case["seed"],
                                 algorithm=case["algorithm"], init=lat)
@@ -79,7 +93,7 @@ def test_int8_identity_cases(oracle_mod, case):
     np.testing.assert_array_equal(sim.get_lattice(), case["final"])
 
 
-def test_int8_set_beta_split(oracle_mod):
+def test_int8_set_beta_split(oracle_mod, int8_path):
     g = golden("int8_cases.npz")
     lat = oracle_mod.random_lattice((128, 128), 1)
     a = oracle_mod.OracleInt8((128, 128), 0.3, seed=3, init=lat)
@@ -129,7 +143,7 @@ def test_observables_definitions(oracle_mod):
     assert cold.observables() == (1.0, -2.0)
 
 
-def test_c1_int8_L1024(oracle_mod):
+def test_c1_int8_L1024(oracle_mod, int8_path):
     """1024^2 int8 Metropolis at beta_c, seed 1, hot start, 1000 sweeps (the reference: 33 s)."""
     g = golden("c1_int8_L1024.npz")
     shape = (1024, 1024)
@@ -152,7 +166,7 @@ def test_c2_msc(oracle_mod, L):
     np.testing.assert_array_equal(sim.get_lattice(), unpack_lattice(g[f"final{L}"], shape))
 
 
-def test_c3_int8_3d_L64(oracle_mod):
+def test_c3_int8_3d_L64(oracle_mod, int8_path):
     g = golden("c3_int8_3d_L64.npz")
     shape = (64, 64, 64)
     sim = oracle_mod.OracleInt8(shape, float(g["beta"]), seed=0, algorithm="heatbath",
@@ -162,7 +176,7 @@ def test_c3_int8_3d_L64(oracle_mod):
     np.testing.assert_array_equal(sim.get_lattice(), unpack_lattice(g["final"], shape))
 
 
-def test_c4_ensemble_members(oracle_mod):
+def test_c4_ensemble_members(oracle_mod, int8_path):
     g = golden("c4_batch.npz")
     for i in g["picked"]:
         i = int(i)
@@ -172,6 +186,32 @@ def test_c4_ensemble_members(oracle_mod):
         series = sim.sweep(500, measure_every=10)
         np.testing.assert_array_equal(series, g[f"series{i}"])
         np.testing.assert_array_equal(sim.get_lattice(), unpack_lattice(g[f"final{i}"], (L, L)))
+
+
+def test_avx512_half_sweep_equals_the_plain_one(oracle_mod):
+    """Random shapes (rows whose length is not a multiple of 4 sites or of 64, 3D, tiny), both
+    rules, negative beta: the two int8 paths give the same spins and series."""
+    if not oracle_mod.fast_active():
+        pytest.skip("no AVX-512 on this host")
+    rng = np.random.default_rng(11)
+    cases = [((6, 10), "metropolis", 0.3), ((34, 258), "metropolis", -0.3),
+             ((128, 250), "heatbath", -0.2), ((10, 6, 22), "heatbath", 0.25),
+             ((12, 14, 18), "metropolis", 0.22), ((2, 2), "metropolis", 1.0)]
+    cases += [((2 * int(rng.integers(1, 40)), 2 * int(rng.integers(1, 90))),
+               ["metropolis", "heatbath"][i % 2], float(rng.uniform(-0.5, 0.9)))
+              for i in range(10)]
+    try:
+        for shape, alg, beta in cases:
+            lat = oracle_mod.random_lattice(shape, 5)
+            out = []
+            for fast in (False, True):
+                oracle_mod.set_fast(fast)
+                sim = oracle_mod.OracleInt8(shape, beta, seed=2**40 + 9, algorithm=alg, init=lat)
+                out.append((sim.sweep(9, measure_every=3), sim.get_lattice()))
+            np.testing.assert_array_equal(out[0][0], out[1][0], err_msg=str(shape))
+            np.testing.assert_array_equal(out[0][1], out[1][1], err_msg=str(shape))
+    finally:
+        oracle_mod.set_fast(True)
 
 
 def test_beta_c_constant():
