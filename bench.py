@@ -404,6 +404,45 @@ def sequential_plain(jobs) -> tuple[float, list]:
     return time.perf_counter() - t0, out
 
 
+def class_of(job) -> str:
+    if job.variant == "msc":
+        return "msc 2D Metropolis"
+    return f"int8 {len(job.shape)}D {job.algorithm}"
+
+
+def best_kernel_rates(jobs) -> dict:
+    """Per kernel class of ``jobs``: the best single-lattice device-timed rate over the class's
+    three largest shapes (device seeded start, CUDA events around 64..2048 sweeps); smaller
+    shapes are launch-bound and never faster."""
+    from pyising_b200 import autotune
+    from pyising_b200.backend import B200Int8, B200MultiSpin
+
+    shapes: dict[str, set] = {}
+    for j in jobs:
+        shapes.setdefault(class_of(j), set()).add((tuple(j.shape), j.algorithm, j.variant,
+                                                   j.beta))
+    out = {}
+    for cls_name, items in shapes.items():
+        best = 0.0
+        for shape, alg, variant, beta in sorted(items, key=lambda t: -int(np.prod(t[0])))[:3]:
+            cls = B200MultiSpin if variant == "msc" else B200Int8
+            sim = cls(shape, beta, seed=12345, algorithm=alg, init="philox")
+            n = int(max(64, min(2048, 2e9 // int(np.prod(shape)))))
+            autotune._time(sim, 32, 1)
+            best = max(best, autotune._time(sim, n, 2))
+            del sim
+        out[cls_name] = round(best, 1)
+    return out
+
+
+def ratio_bound(jobs, t_seq: float, rates: dict) -> dict:
+    """The largest batched/sequential ratio any batched kernel could reach: the sequential time
+    over the time the jobs' flips take at their class's best single-lattice rate."""
+    t_min = sum(j.n_spins * j.sweeps / (rates[class_of(j)] * 1e9) for j in jobs)
+    return {"class_best_flips_per_ns": rates, "best_kernel_s": round(t_min, 3),
+            "ratio_upper_bound": round(t_seq / t_min, 3)}
+
+
 def c4_oracle_check(jobs, results) -> dict:
     """Every member's series and final lattice against the oracle (all host threads), after
     the timed region: the checker, not a measured path."""
@@ -456,6 +495,7 @@ def run_batched_ensemble(check_oracle: bool = True) -> dict:
             "batched_flips_per_ns": round(flips / t_batch / 1e9, 2),
             "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
             "speedup": round(t_seq / t_batch, 3), "bit_identical": bool(same),
+            "bound": ratio_bound(jobs, t_seq, best_kernel_rates(jobs)),
             "oracle_identical": oracle_check["identical"] if oracle_check else None,
             "oracle_check": oracle_check,
             "tuned_batch_knobs": tuned["config"],
@@ -534,6 +574,7 @@ def run_served_stream(n_jobs: int, baseline_jobs: int | None = None) -> dict:
             "sequential_s": round(t_seq, 3),
             "sequential_flips_per_ns": round(seq_rate, 2),
             "speedup": round(served_rate / seq_rate, 3),
+            "bound": ratio_bound(jobs[:nb], t_seq, best_kernel_rates(jobs[:nb])),
             "latency_p50_s": round(float(np.percentile(lat, 50)), 4),
             "latency_p99_s": round(float(np.percentile(lat, 99)), 4),
             "latency_max_s": round(float(lat.max()), 4),
