@@ -341,6 +341,18 @@ public:
         if ((int64_t)j->device_bytes > budget_)
             return fail(ISING_ERR_NOMEM, "job needs %zu device bytes, over the %lld-byte budget",
                         j->device_bytes, (long long)budget_);
+        // the pinned host buffers of the results are taken now, on the submitting thread:
+        // page-locking memory while the job finishes would stall the sweeps in flight
+        cudaError_t e = cudaSuccess;
+        if (j->series_pairs)
+            e = pinned_get((void**)&j->h_series, j->series_pairs * 2 * sizeof(long long));
+        if (e == cudaSuccess && spec.keep_lattice)
+            e = pinned_get((void**)&j->h_lattice, (size_t)j->rows * 2 * j->lh);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            free_job(*j);
+            return fail(ISING_ERR_NOMEM, "pinned result buffers of a job");
+        }
         j->id = ++last_id_;
         j->t_submit = Clock::now();
         *id = j->id;
@@ -959,14 +971,14 @@ private:
         cudaError_t e = cudaSuccess;
         if (j.series_pairs) {
             const size_t sb = j.series_pairs * 2 * sizeof(long long);
-            e = pinned_get((void**)&j.h_series, sb);
+            if (!j.h_series) e = pinned_get((void**)&j.h_series, sb);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(j.h_series, j.d_series, sb, cudaMemcpyDeviceToHost, stream_);
         }
         if (e == cudaSuccess && j.spec.keep_lattice) {
             const size_t full = (size_t)j.rows * 2 * j.lh;
             int8_t* stage = nullptr;
-            e = pinned_get((void**)&j.h_lattice, full);
+            if (!j.h_lattice) e = pinned_get((void**)&j.h_lattice, full);
             if (e == cudaSuccess) e = dev_alloc((void**)&stage, full);
             if (e == cudaSuccess) {
                 if (j.spec.variant == ISING_VARIANT_MSC)

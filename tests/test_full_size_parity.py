@@ -35,7 +35,8 @@ def test_headline_msc_16384_1000_sweeps(oracle_mod):
     st = sim.state()
     series = sim.sweep_measured(1000, 100)
     ref = oracle_mod.OracleMultiSpin(shape, BETA_C_2D, seed=7, init="cold")
-    ref.w = [np.ascontiguousarray(st["c0"]), np.ascontiguousarray(st["c1"])]
+    # copies: the oracle sweeps its arrays in place, and the unmeasured run below starts from st
+    ref.w = [np.array(st["c0"], copy=True), np.array(st["c1"], copy=True)]
     ref_series = ref.sweep(1000, measure_every=100)
     np.testing.assert_array_equal(series, ref_series)
     w0, w1 = sim.colour_arrays()
