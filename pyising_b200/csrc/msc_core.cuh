@@ -335,6 +335,17 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
 // the range schedule.  Random numbers, levels and their order are the reference's, so the
 // results are identical.
 
+#ifndef ISING_STRIP_SPLIT
+#define ISING_STRIP_SPLIT 0
+#endif
+#ifndef ISING_STRIP_SHARED_MASKS
+#define ISING_STRIP_SHARED_MASKS 0
+#endif
+// Philox products as separate high/low multiplies; intake level masks read from the block's
+// shared table instead of derived from the thresholds in uniform registers.
+constexpr bool kStripSplit = ISING_STRIP_SPLIT != 0;
+constexpr bool kStripSharedMasks = ISING_STRIP_SHARED_MASKS != 0;
+
 // Pair sums of two anti-aligned flags: s = exactly one, c = both.
 struct HalfSlices {
     u32 a1, a2;  // exactly one / two or more anti-aligned neighbours
@@ -412,9 +423,10 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             const u32 w = (u32)((long long)yc * nw + x);
 #pragma unroll
             for (int b = 0; b < K; ++b) {
-                const u32x4 r = philox4x32_10(w, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
-                block_levels(r, level_masks(p.thr4, p.thr8, (u32)b), sl.a1, sh.a1, undl, undh,
-                             accl, acch);
+                const u32x4 r =
+                    philox4x32_10<kStripSplit>(w, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
+                block_levels(r, kStripSharedMasks ? lvmask[b] : level_masks(p.thr4, p.thr8, (u32)b),
+                             sl.a1, sh.a1, undl, undh, accl, acch);
             }
             const u32 resl = (u32)o ^ sl.a2 ^ accl, resh = (u32)(o >> 32) ^ sh.a2 ^ acch;
             const bool keep = (undl | undh) != 0;
@@ -444,7 +456,7 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             __syncwarp();
             u32 undl = (u32)und, undh = (u32)(und >> 32), accl = 0, acch = 0;
             if (act) {
-                const u32x4 r = philox4x32_10(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
+                const u32x4 r = philox4x32_10<kStripSplit>(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
                 block_levels(r, lvmask[lp], (u32)a1, (u32)(a1 >> 32), undl, undh, accl, acch);
                 ++lp;
             }
