@@ -56,7 +56,7 @@ DESCRIPTION = {
                    "with (E, M) every 10 sweeps",
 }
 MEASURE_EVERY = {"int8_3d_256": 10}
-KERNEL = {"msc": "msc_half_queue_kernel", "int8": "int8_half_kernel"}
+KERNEL = {"msc": "msc_strip_kernel", "int8": "int8_half_kernel"}
 
 
 # ------------------------------------------------------------------------- helpers -------
@@ -411,36 +411,51 @@ def class_of(job) -> str:
 
 
 def best_kernel_rates(jobs) -> dict:
-    """Per kernel class of ``jobs``: the best single-lattice device-timed rate over the class's
-    three largest shapes (device seeded start, CUDA events around 64..2048 sweeps); smaller
-    shapes are launch-bound and never faster."""
+    """Per kernel class of ``jobs``: the autotuned single-lattice rate of the class's largest
+    shape (device-timed; smaller shapes are launch-bound and never faster), and the class's
+    Philox calls per update (0.25 for int8; the measured calls per word / 64 for msc)."""
     from pyising_b200 import autotune
-    from pyising_b200.backend import B200Int8, B200MultiSpin
+    from pyising_b200.backend import B200MultiSpin
 
-    shapes: dict[str, set] = {}
+    largest: dict[str, tuple] = {}
     for j in jobs:
-        shapes.setdefault(class_of(j), set()).add((tuple(j.shape), j.algorithm, j.variant,
-                                                   j.beta))
-    out = {}
-    for cls_name, items in shapes.items():
-        best = 0.0
-        for shape, alg, variant, beta in sorted(items, key=lambda t: -int(np.prod(t[0])))[:3]:
-            cls = B200MultiSpin if variant == "msc" else B200Int8
-            sim = cls(shape, beta, seed=12345, algorithm=alg, init="philox")
-            n = int(max(64, min(2048, 2e9 // int(np.prod(shape)))))
-            autotune._time(sim, 32, 1)
-            best = max(best, autotune._time(sim, n, 2))
+        k = class_of(j)
+        if k not in largest or j.n_spins > int(np.prod(largest[k][0])):
+            largest[k] = (tuple(j.shape), j.algorithm, j.variant, j.beta)
+    rates, calls = {}, {}
+    for k, (shape, alg, variant, beta) in largest.items():
+        rates[k] = round(autotune.tune(variant, shape, alg, beta, save=False)["flips_per_ns"], 1)
+        if variant == "msc":
+            sim = B200MultiSpin(shape, beta, seed=12345, init="philox")
+            calls[k] = round(sim.philox_calls_per_word(2) / 64.0, 5)
             del sim
-        out[cls_name] = round(best, 1)
-    return out
+        else:
+            calls[k] = 0.25
+    return {"flips_per_ns": rates, "philox_calls_per_update": calls}
 
 
-def ratio_bound(jobs, t_seq: float, rates: dict) -> dict:
-    """The largest batched/sequential ratio any batched kernel could reach: the sequential time
-    over the time the jobs' flips take at their class's best single-lattice rate."""
-    t_min = sum(j.n_spins * j.sweeps / (rates[class_of(j)] * 1e9) for j in jobs)
-    return {"class_best_flips_per_ns": rates, "best_kernel_s": round(t_min, 3),
-            "ratio_upper_bound": round(t_seq / t_min, 3)}
+def ratio_bound(jobs, t_seq: float, best: dict, t_batched: float) -> dict:
+    """How far the batched/sequential ratio can go.  ``at_best_kernel``: the sequential time over
+    the time the jobs' flips take at their class's best rate (the autotuned single-lattice rate,
+    or the batched run's own rate when that is higher); ``at_philox_ceiling``: over the time
+    the Philox blocks alone take at the measured Philox rate, which no kernel can beat."""
+    from pyising_b200._lib import philox_rate
+
+    flips = sum(j.n_spins * j.sweeps for j in jobs)
+    rates = best["flips_per_ns"]
+    t_kernel = sum(j.n_spins * j.sweeps / (rates[class_of(j)] * 1e9) for j in jobs)
+    t_kernel = min(t_kernel, t_batched)
+    rate = philox_rate(0, 512, 5)
+    t_philox = sum(j.n_spins * j.sweeps * best["philox_calls_per_update"][class_of(j)]
+                   for j in jobs) / (rate * 1e9)
+    return {"class_best_flips_per_ns": rates,
+            "philox_calls_per_update": best["philox_calls_per_update"],
+            "philox_calls_per_ns": round(rate, 1),
+            "best_kernel_s": round(t_kernel, 3),
+            "at_best_kernel": round(t_seq / t_kernel, 3),
+            "philox_s": round(t_philox, 3),
+            "at_philox_ceiling": round(t_seq / t_philox, 3),
+            "best_kernel_flips_per_ns": round(flips / t_kernel / 1e9, 1)}
 
 
 def c4_oracle_check(jobs, results) -> dict:
@@ -495,7 +510,7 @@ def run_batched_ensemble(check_oracle: bool = True) -> dict:
             "batched_flips_per_ns": round(flips / t_batch / 1e9, 2),
             "sequential_flips_per_ns": round(flips / t_seq / 1e9, 2),
             "speedup": round(t_seq / t_batch, 3), "bit_identical": bool(same),
-            "bound": ratio_bound(jobs, t_seq, best_kernel_rates(jobs)),
+            "bound": ratio_bound(jobs, t_seq, best_kernel_rates(jobs), t_batch),
             "oracle_identical": oracle_check["identical"] if oracle_check else None,
             "oracle_check": oracle_check,
             "tuned_batch_knobs": tuned["config"],
@@ -574,7 +589,8 @@ def run_served_stream(n_jobs: int, baseline_jobs: int | None = None) -> dict:
             "sequential_s": round(t_seq, 3),
             "sequential_flips_per_ns": round(seq_rate, 2),
             "speedup": round(served_rate / seq_rate, 3),
-            "bound": ratio_bound(jobs[:nb], t_seq, best_kernel_rates(jobs[:nb])),
+            "bound": ratio_bound(jobs[:nb], t_seq, best_kernel_rates(jobs[:nb]),
+                                 served_s * base_flips / flips),
             "latency_p50_s": round(float(np.percentile(lat, 50)), 4),
             "latency_p99_s": round(float(np.percentile(lat, 99)), 4),
             "latency_max_s": round(float(lat.max()), 4),
