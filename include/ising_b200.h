@@ -148,8 +148,8 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
  * 1 = no tiles: one union-find in global memory, else 32..6144); the labels are the same for
  * every value. */
 #define ISING_KNOB_CLUSTER_TILE 7
-/* msc schedule: 0 = automatic (strips where each row holds 128 or more words, a multiple of
- * 32), 1 = word ranges per warp, 2..7 = 32-word column strips walked down a band of rows two
+/* msc schedule: 0 = automatic (strips where each row holds a multiple of 32 words, ranges
+ * elsewhere), 1 = word ranges per warp, 2..7 = 32-word column strips walked down a band of rows two
  * rows per step, with (Philox blocks per word before the work stack, resident blocks of 256
  * threads the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4). */
 #define ISING_KNOB_MSC_KERNEL 9

@@ -164,9 +164,9 @@ cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int s
 {
     // the strip schedule needs rows of whole 32-word strips and word indices below 2^32
     const bool strip_ok = p.nw % 32 == 0 && (long long)p.rows * p.nw <= 0xFFFFFFFFll;
-    // automatic: the strips (4 intake blocks, registers for 2 blocks per SM) from 128 words per
-    // row on; the word ranges below, where rows hold too few strips to fill the bands
-    if (kernel == 0) kernel = strip_ok && p.nw >= 128 ? 2 : 1;
+    // automatic: the strips (4 intake blocks, registers for 2 blocks per SM) wherever the rows
+    // hold whole 32-word strips, the word ranges elsewhere
+    if (kernel == 0) kernel = strip_ok ? 2 : 1;
     if (update && !p.stats && strip_ok && kernel >= 2) {
         switch (kernel) {
         case 2: return strip_launch<4, 2>(p, sm_count, waves, st);
