@@ -153,9 +153,6 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
  * rows per step, with (Philox blocks per word before the work stack, resident blocks of 256
  * threads the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4). */
 #define ISING_KNOB_MSC_KERNEL 9
-/* int8 half-sweeps: 1 = warps claim 32 slots (band, chunk column) at a time from a counter
- * until none is left, one resident wave of blocks; 0 = grid-stride slots. */
-#define ISING_KNOB_INT8_CLAIM 10
 /* Test hook of the bounded union-find loops (0 = off): 1 makes every cluster labeling write a
  * two-site cycle into the labels (sites 0 and S) after the unions, so the root walks that follow
  * run out of their step budgets and the call returns ISING_ERR_TIMEOUT, with the context intact.

@@ -6,8 +6,6 @@ by site, sweep and colour, and every schedule visits the same sites with the sam
 * ``band``          int8: rows of one plane a thread walks while the opposite colour's rows
                     slide through its registers (the halo reuse depth); 0 = occupancy default;
 * ``chunk_width``   int8: bytes per thread and row, 16, 8 or 4 (4, 2 or 1 words of 4 sites);
-* ``int8_claim``    int8: warps claim 32 slots at a time from a counter (one resident wave of
-                    blocks) instead of taking them grid-stride;
 * ``blocks_per_sm`` grid size in blocks of 256 threads per SM;
 * ``msc_kernel``    msc: schedule: word ranges per warp, or 32-word column strips walked down a
                     band of rows with 4 or 3 Philox blocks per word at intake and registers
@@ -42,9 +40,9 @@ from . import _lib
 from ._lib import check, lib
 
 KNOBS = {"band": 1, "chunk_width": 2, "blocks_per_sm": 3, "msc_waves": 4, "graph_chunk": 5,
-         "msc_kernel": 9, "int8_claim": 10}
+         "msc_kernel": 9}
 DEFAULTS = {"band": 0, "chunk_width": 16, "blocks_per_sm": 8, "msc_waves": 1, "graph_chunk": 32,
-            "msc_kernel": 0, "int8_claim": 0, "schedule": "auto"}
+            "msc_kernel": 0, "schedule": "auto"}
 
 _lock = threading.Lock()
 _cache_mem: dict[Path, dict] = {}  # cache file contents by path, read once per process
@@ -80,7 +78,6 @@ def search_space(variant: str, shape, algorithm: str = "metropolis") -> dict[str
     if variant == "int8":
         space["band"] = [0, 1, 2, 4, 8, 16]
         space["chunk_width"] = [16, 4] + ([8] if lh % 8 == 0 else [])
-        space["int8_claim"] = [0, 1]
     else:
         # 0 = automatic; 1 = word ranges; 2..7 = column strips with (intake blocks, register
         # bound) variants, where every row holds whole 32-word strips

@@ -354,16 +354,14 @@ int ising_create(int ndim, const int64_t* shape, int variant, int algorithm, uin
                         cudaGetErrorString(e));
         }
     }
-    // [0,1] observables, [2,3] msc call statistics, [6,7] graph control block, [8] the int8
-    // kernels' slot-claim counters (two u32)
-    e = pool_alloc(device, (void**)&h->d_acc, 9 * sizeof(unsigned long long), h->stream);
+    e = pool_alloc(device, (void**)&h->d_acc, 8 * sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         h->d_acc = nullptr;
         ising_destroy(h);
         return fail(ISING_ERR_NOMEM, "allocation of the accumulators failed");
     }
-    e = cudaMemsetAsync(h->d_acc, 0, 9 * sizeof(unsigned long long), h->stream);
+    e = cudaMemsetAsync(h->d_acc, 0, 8 * sizeof(unsigned long long), h->stream);
     // the arrays are usable from any stream once their allocation has completed
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
@@ -620,10 +618,6 @@ int ising_set_knob(ising_sim* h, int knob, int value)
         if (value < 0 || value > 7) return fail(ISING_ERR_INVALID, "msc kernel must be 0..7");
         h->msc_kernel = value;
         break;
-    case ISING_KNOB_INT8_CLAIM:
-        if (value != 0 && value != 1) return fail(ISING_ERR_INVALID, "int8 claim is 0 or 1");
-        h->int8_claim = value;
-        break;
     case ISING_KNOB_TEST_LABEL_CYCLE:
         if (value != 0 && value != 1) return fail(ISING_ERR_INVALID, "test hook is 0 or 1");
         h->test_label_cycle = value;
@@ -646,7 +640,6 @@ int ising_get_knob(ising_sim* h, int knob, int* value)
     case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
     case ISING_KNOB_CLUSTER_TILE: *value = h->cluster_tile; break;
     case ISING_KNOB_MSC_KERNEL: *value = h->msc_kernel; break;
-    case ISING_KNOB_INT8_CLAIM: *value = h->int8_claim; break;
     case ISING_KNOB_TEST_LABEL_CYCLE: *value = h->test_label_cycle; break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }
@@ -994,7 +987,6 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
         for (int i = 0; i < 7; ++i) p.table[i] = h->table[i];
         p.meas = meas;
         p.ctl = ctl;
-        p.claim = h->int8_claim ? reinterpret_cast<unsigned int*>(h->d_acc + 8) : nullptr;
         e = launch_int8_half(h->ndim, h->rule, p, h->max_blocks, h->sm_count, h->stream);
     }
     if (e != cudaSuccess) return cuda_fail(e, "half-sweep launch");

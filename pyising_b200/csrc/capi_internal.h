@@ -40,7 +40,6 @@ struct ising_sim {
     int blocks_per_sm = 8;
     int msc_waves = 1;                  // msc: warp ranges per resident warp
     int msc_kernel = 0;                 // msc: schedule (ISING_KNOB_MSC_KERNEL)
-    int int8_claim = 0;                 // int8: slots claimed by warps (ISING_KNOB_INT8_CLAIM)
     int64_t graph_chunk = 32;           // sweeps per captured graph of an unmeasured run
     // Captured chunks of `sweeps` sweeps (one measurement at the end when `measured`), replayed
     // with the sweep counter and series slot in d_acc[6], d_acc[7].

@@ -140,9 +140,6 @@ struct Int8Half {
     // Graph-replay control block, or nullptr: when set, the sweep counter is ctl[0] + t and the
     // accumulators are meas + 2 * ctl[1] (a captured chunk of sweeps advances ctl itself).
     const unsigned long long* ctl;
-    // Dynamic slot claiming, or nullptr (grid-stride slots): claim[0] is the next unclaimed
-    // slot, claim[1] counts finished blocks; the last block to finish resets both to zero.
-    unsigned int* claim = nullptr;
 };
 
 // Parameters of one packed (msc) half-sweep launch over (rows, nw) uint64 words.

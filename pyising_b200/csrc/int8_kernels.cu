@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
     long long m_acc = 0, e_acc = 0;
     const u32 cpr = (u32)p.cpr, bpp = (u32)p.bpp;
     const u32 nslots = (u32)p.lz * bpp * cpr;
-    auto run_slot = [&](u32 slot) {
+    for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
+         slot += gridDim.x * blockDim.x) {
         const u32 band = fast_div(slot, cpr, p.cpr_magic);
         const int j0 = (int)(slot - band * cpr) * V;
         int z = 0, yb = (int)band;
@@ -38,31 +39,6 @@ __global__ void __launch_bounds__(256, 4) int8_half_kernel(const Int8Half p_in)
         const int y0 = yb * p.band;
         const int y1 = y0 + p.band < p.ly ? y0 + p.band : p.ly;
         int8_band<V, NDIM, RULE, MIXED, MEAS>(p, z, y0, y1, j0, stab, m_acc, e_acc);
-    };
-    if (p.claim) {
-        // a warp claims 32 consecutive slots at a time until none is left, so every SM stays
-        // busy to the end of the launch instead of the grid-stride share of its blocks
-        const int lane = threadIdx.x & 31;
-        while (true) {
-            u32 base = 0;
-            if (lane == 0) base = atomicAdd(p.claim, 32u);
-            base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            if (base >= nslots) break;
-            if (base + (u32)lane < nslots) run_slot(base + (u32)lane);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            if (atomicAdd(p.claim + 1, 1u) == gridDim.x - 1) {  // the last block: reset
-                p.claim[0] = 0u;
-                p.claim[1] = 0u;
-                __threadfence();
-            }
-        }
-    } else {
-        for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
-             slot += gridDim.x * blockDim.x)
-            run_slot(slot);
     }
     if constexpr (MEAS) block_accumulate2(m_acc, e_acc, p.meas);
 }
@@ -118,8 +94,6 @@ unsigned int8_band_geometry(Int8Half& p, int max_blocks, int sm_count)
     p.bpp_magic = fast_div_magic((u32)p.bpp, (unsigned long long)p.lz * p.bpp);
     unsigned long long g = (nslots + 255) / 256;
     if (g > (unsigned long long)max_blocks) g = (unsigned long long)max_blocks;
-    // claimed slots: one resident wave (4 blocks of 256 per SM) is enough
-    if (p.claim && g > 4ull * (unsigned long long)sm_count) g = 4ull * (unsigned long long)sm_count;
     return (unsigned)(g < 1 ? 1 : g);
 }
 
