@@ -151,8 +151,7 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
 /* msc schedule: 0 = automatic (strips where each row holds a multiple of 32 words, ranges
  * elsewhere), 1 = word ranges per warp, 2..7 = 32-word column strips walked down a band of rows two
  * rows per step, with (Philox blocks per word before the work stack, resident blocks of 256
- * threads the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4);
- * 8 / 9 = 4 / 3 intake blocks in blocks of 128 threads, registers bounded for 5 per SM. */
+ * threads the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4). */
 #define ISING_KNOB_MSC_KERNEL 9
 /* Test hook of the bounded union-find loops (0 = off): 1 makes every cluster labeling write a
  * two-site cycle into the labels (sites 0 and S) after the unions, so the root walks that follow

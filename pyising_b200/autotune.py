@@ -9,7 +9,7 @@ by site, sweep and colour, and every schedule visits the same sites with the sam
 * ``blocks_per_sm`` grid size in blocks of 256 threads per SM;
 * ``msc_kernel``    msc: schedule: word ranges per warp, or 32-word column strips walked down a
                     band of rows with 4 or 3 Philox blocks per word at intake and registers
-                    bounded for 2, 3 or 4 resident blocks of 8 warps or 5 of 4 warps;
+                    bounded for 2, 3 or 4 resident blocks;
 * ``msc_waves``     msc: warps per resident warp (ranges or strip bands of the work-stack kernels);
 * ``graph_chunk``   sweeps per captured CUDA graph of an unmeasured run;
 * ``schedule``      ``"auto"`` (graphs), ``"launches"``, ``"persistent"`` or ``"temporal"``
@@ -81,7 +81,7 @@ def search_space(variant: str, shape, algorithm: str = "metropolis") -> dict[str
     else:
         # 0 = automatic; 1 = word ranges; 2..7 = column strips with (intake blocks, register
         # bound) variants, where every row holds whole 32-word strips
-        space["msc_kernel"] = [0, 1] + ([2, 3, 4, 5, 6, 7, 8, 9] if (lh // 64) % 32 == 0 else [])
+        space["msc_kernel"] = [0, 1] + ([2, 3, 4, 5, 6, 7] if (lh // 64) % 32 == 0 else [])
         space["msc_waves"] = [1, 2, 4]
     space["blocks_per_sm"] = [8, 4, 16]
     if variant == "int8" and len(shape) == 2:

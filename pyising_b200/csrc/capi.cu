@@ -615,7 +615,7 @@ int ising_set_knob(ising_sim* h, int knob, int value)
         h->cluster_tile = value;
         break;
     case ISING_KNOB_MSC_KERNEL:
-        if (value < 0 || value > 9) return fail(ISING_ERR_INVALID, "msc kernel must be 0..9");
+        if (value < 0 || value > 7) return fail(ISING_ERR_INVALID, "msc kernel must be 0..7");
         h->msc_kernel = value;
         break;
     case ISING_KNOB_TEST_LABEL_CYCLE:

@@ -86,8 +86,7 @@ cudaError_t launch_int8_half(int ndim, int rule, const Int8Half& p, int max_bloc
                              cudaStream_t st);
 // kernel: 0 = automatic (the strip schedule where the rows hold whole 32-word strips), 1 = the
 // range schedule, 2..7 = the strip schedule with (Philox blocks per word at intake, resident
-// blocks the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4); 8 / 9 =
-// 4 / 3 intake blocks in blocks of 4 warps, registers bounded for 5 blocks per SM.
+// blocks the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4).
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int sm_count,
                             int waves, cudaStream_t st, int kernel = 0);
 cudaError_t launch_int8_split(const int8_t* full, int8_t* c0, int8_t* c1, long long rows,

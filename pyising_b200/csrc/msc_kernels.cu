@@ -55,19 +55,19 @@ __global__ void __launch_bounds__(kQueueWarps * 32, ISING_MSC_MIN_BLOCKS)
 
 // Strip schedule: warp g walks rows [band (g / strips), band (g / strips + 1)) of strip
 // g % strips; K Philox blocks per word at intake; registers bounded for MINB resident blocks.
-template <bool MEAS, int K, int MINB, int WPB = kQueueWarps>
-__global__ void __launch_bounds__(WPB * 32, MINB)
+template <bool MEAS, int K, int MINB>
+__global__ void __launch_bounds__(kQueueWarps * 32, MINB)
     msc_strip_kernel(const MscHalf p_in, int strips, int band)
 {
     MscHalf p = p_in;
-    __shared__ StripSlots q_all[WPB];
+    __shared__ StripSlots q_all[kQueueWarps];
     __shared__ uint4 lvmask[16];
     if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
     pdl_wait();  // the previous half-sweep has completed
     pdl_trigger();
     resolve_ctl(p);
     __syncthreads();
-    const int g = blockIdx.x * WPB + (threadIdx.x >> 5);
+    const int g = blockIdx.x * kQueueWarps + (threadIdx.x >> 5);
     const int strip = g % strips;
     const int y0 = (g / strips) * band;
     const int y1 = min(y0 + band, p.rows);
@@ -117,7 +117,7 @@ static int queue_blocks_per_sm()
 
 int msc_nw_shift(int nw) { return (nw & (nw - 1)) == 0 ? __builtin_ctz((unsigned)nw) : -1; }
 
-template <bool MEAS, int K, int MINB, int WPB>
+template <bool MEAS, int K, int MINB>
 static int strip_blocks_per_sm()
 {
     static int cached[64] = {};
@@ -126,8 +126,8 @@ static int strip_blocks_per_sm()
     if (dev < 0 || dev >= 64) dev = 0;
     if (!cached[dev]) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_strip_kernel<MEAS, K, MINB, WPB>,
-                                                          WPB * 32, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_strip_kernel<MEAS, K, MINB>,
+                                                          kQueueWarps * 32, 0) != cudaSuccess ||
             b < 1) {
             cudaGetLastError();
             b = 2;
@@ -137,26 +137,26 @@ static int strip_blocks_per_sm()
     return cached[dev];
 }
 
-template <bool MEAS, int K, int MINB, int WPB>
+template <bool MEAS, int K, int MINB>
 static cudaError_t launch_strip(const MscHalf& p, int sm_count, int waves, cudaStream_t st)
 {
     const int strips = p.nw / 32;
     const long long units = (long long)p.rows * strips;  // (row, strip) steps
     const long long warps = (long long)(sm_count > 0 ? sm_count : 1) *
-                            strip_blocks_per_sm<MEAS, K, MINB, WPB>() * WPB * (waves > 0 ? waves : 1);
+                            strip_blocks_per_sm<MEAS, K, MINB>() * kQueueWarps * (waves > 0 ? waves : 1);
     long long band = (units + warps - 1) / warps;
     if (band < 1) band = 1;
     const long long nwarps = (long long)strips * ((p.rows + band - 1) / band);
-    const unsigned blocks = (unsigned)((nwarps + WPB - 1) / WPB);
-    return launch_pdl(msc_strip_kernel<MEAS, K, MINB, WPB>, dim3(blocks), dim3(WPB * 32), st, p,
+    const unsigned blocks = (unsigned)((nwarps + kQueueWarps - 1) / kQueueWarps);
+    return launch_pdl(msc_strip_kernel<MEAS, K, MINB>, dim3(blocks), dim3(kQueueWarps * 32), st, p,
                       strips, (int)band);
 }
 
-template <int K, int MINB, int WPB = kQueueWarps>
+template <int K, int MINB>
 static cudaError_t strip_launch(const MscHalf& p, int sm_count, int waves, cudaStream_t st)
 {
-    return p.meas ? launch_strip<true, K, MINB, WPB>(p, sm_count, waves, st)
-                  : launch_strip<false, K, MINB, WPB>(p, sm_count, waves, st);
+    return p.meas ? launch_strip<true, K, MINB>(p, sm_count, waves, st)
+                  : launch_strip<false, K, MINB>(p, sm_count, waves, st);
 }
 
 cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int sm_count,
@@ -174,9 +174,7 @@ cudaError_t launch_msc_half(bool update, const MscHalf& p, int max_blocks, int s
         case 4: return strip_launch<4, 4>(p, sm_count, waves, st);
         case 5: return strip_launch<3, 2>(p, sm_count, waves, st);
         case 6: return strip_launch<3, 3>(p, sm_count, waves, st);
-        case 7: return strip_launch<3, 4>(p, sm_count, waves, st);
-        case 8: return strip_launch<4, 5, 4>(p, sm_count, waves, st);
-        default: return strip_launch<3, 5, 4>(p, sm_count, waves, st);
+        default: return strip_launch<3, 4>(p, sm_count, waves, st);
         }
     }
     if (update && !p.stats) {

@@ -14,7 +14,7 @@ KNOB_MSC_KERNEL = 9
 
 
 @pytest.mark.parametrize("shape", [(64, 4096), (34, 8192), (16, 12288), (128, 1024)], ids=str)
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_msc_schedules_match_the_oracle(oracle_mod, shape, kernel):
     from pyising_b200._lib import check, lib
     from pyising_b200.backend import B200MultiSpin
@@ -39,6 +39,6 @@ def test_msc_kernel_knob_range():
     from pyising_b200.backend import B200MultiSpin
 
     sim = B200MultiSpin((16, 256), 0.4, init="cold")
-    for bad in (-1, 10):
+    for bad in (-1, 8):
         with pytest.raises(ValueError):
             check(lib().ising_set_knob(sim._h, KNOB_MSC_KERNEL, bad), "set_knob")
