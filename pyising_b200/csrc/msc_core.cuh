@@ -391,7 +391,7 @@ struct StripSlots {
 // One pass over the stack: a Philox block for each of up to 32 entries at its own level pair;
 // the result word of an entry already holds every decision made so far.
 __device__ __forceinline__ void strip_pop(const MscHalf& p, StripSlots& q, int& n,
-                                          const uint4* lvmask)
+                                          const uint4* lvmask, u32 wg)
 {
     const int lane = threadIdx.x & 31;
     const u32 lt = (1u << lane) - 1u;
@@ -406,7 +406,7 @@ __device__ __forceinline__ void strip_pop(const MscHalf& p, StripSlots& q, int& 
     __syncwarp();
     u32 undl = (u32)und, undh = (u32)(und >> 32), accl = 0, acch = 0;
     if (act) {
-        const u32x4 r = philox4x32_10<true>(idx, p.t, p.color, 1u + lp, p.k0, p.k1);
+        const u32x4 r = philox4x32_10<true>(wg + idx, p.t, p.color, 1u + lp, p.k0, p.k1);
         block_levels(r, lvmask[lp], (u32)a1, (u32)(a1 >> 32), undl, undh, accl, acch);
         ++lp;
     }
@@ -427,9 +427,13 @@ __device__ __forceinline__ void strip_pop(const MscHalf& p, StripSlots& q, int& 
 }
 
 // The warp updates rows [y0, y1) of strip `strip` (words 32 strip .. 32 strip + 31 of a row).
-template <int K>
+// SLAB: the lattice is a slab of a bigger one (SlabOffset): Philox word indices are so.w0 + the
+// local index, row parities those of the global rows, and rows -1 and `rows` of the opposite
+// colour are read from so.lo and so.hi instead of wrapping.
+template <int K, bool SLAB = false>
 __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int y0, int y1,
-                                               StripSlots& q, const uint4* lvmask)
+                                               StripSlots& q, const uint4* lvmask,
+                                               const SlabOffset& so = {0, 0, nullptr, nullptr})
 {
     const int lane = threadIdx.x & 31;
     const u32 lt = (1u << lane) - 1u;
@@ -437,21 +441,29 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
     const int x = strip * 32 + lane;
     const int xr = x + 1 == nw ? 0 : x + 1, xl = x == 0 ? nw - 1 : x - 1;
     const u64* other = p.other;
-    const int odd0 = (int)p.color & 1;  // parity of row 0 for this colour
-    u64 up = __ldg(other + (long long)(y0 == 0 ? rows - 1 : y0 - 1) * nw + x);
-    u64 c = __ldg(other + (long long)y0 * nw + x);
+    const u32 wg = SLAB ? (u32)so.w0 : 0u;
+    const int odd0 = ((SLAB ? so.par0 : 0) + (int)p.color) & 1;  // parity of local row 0
+    // opposite-colour row r, r in [-1, rows]
+    auto orow = [&](int r) -> const u64* {
+        if constexpr (SLAB) {
+            if (r < 0) return so.lo;
+            if (r >= rows) return so.hi;
+        } else {
+            r = r < 0 ? rows - 1 : (r >= rows ? 0 : r);
+        }
+        return other + (long long)r * nw;
+    };
+    u64 up = __ldg(orow(y0 - 1) + x);
+    u64 c = __ldg(orow(y0) + x);
     u64 f_o0 = 0, f_o1 = 0, f_d1 = 0, f_d2 = 0, f_s0 = 0, f_s1 = 0;
     auto fetch = [&](int y) {
-        const long long rb = (long long)y * nw;
-        const int ya = y + 1 == rows ? 0 : y + 1;
-        f_o0 = p.own[rb + x];
-        f_d1 = __ldg(other + (long long)ya * nw + x);
-        f_s0 = __ldg(other + rb + (((y + odd0) & 1) ? xr : xl));
+        f_o0 = p.own[(long long)y * nw + x];
+        f_d1 = __ldg(orow(y + 1) + x);
+        f_s0 = __ldg(orow(y) + (((y + odd0) & 1) ? xr : xl));
         if (y + 1 < y1) {
-            const int yb = ya + 1 == rows ? 0 : ya + 1;
-            f_o1 = p.own[(long long)ya * nw + x];
-            f_d2 = __ldg(other + (long long)yb * nw + x);
-            f_s1 = __ldg(other + (long long)ya * nw + (((ya + odd0) & 1) ? xr : xl));
+            f_o1 = p.own[(long long)(y + 1) * nw + x];
+            f_d2 = __ldg(orow(y + 2) + x);
+            f_s1 = __ldg(orow(y + 1) + (((y + 1 + odd0) & 1) ? xr : xl));
         }
     };
     int y = y0;
@@ -482,9 +494,9 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             for (int b = 0; b < K; ++b) {
                 const uint4 m = lvmask[b];
                 const u32x4 ra =
-                    philox4x32_10<true>(wa, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
+                    philox4x32_10<true>(wg + wa, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
                 const u32x4 rb =
-                    philox4x32_10<true>(wb, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
+                    philox4x32_10<true>(wg + wb, p.t, p.color, 1u + (u32)b, p.k0, p.k1);
                 block_levels(ra, m, al.a1, ah.a1, ual, uah, aal, aah);
                 block_levels(rb, m, bl.a1, bh.a1, ubl, ubh, abl, abh);
             }
@@ -515,7 +527,7 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             n += __popc(kmb);
             __syncwarp();
         } else if (n > 0) {
-            strip_pop(p, q, n, lvmask);
+            strip_pop(p, q, n, lvmask, wg);
         } else {
             break;
         }

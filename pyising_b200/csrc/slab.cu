@@ -48,6 +48,7 @@ struct ising_slab {
     int sm_count = 148;
     int max_blocks = 148 * 8;
     int queue_blocks = 2;  // resident blocks per SM of the msc work-stack kernel
+    int strip_blocks = 2;  // ... of the msc strip kernel
     // Neighbouring slabs whose edge rows the kernels read in place of this slab's halos
     // (ising_slab_set_peer), per colour; nullptr: the own halo rows.
     const char* peer_lo[2] = {nullptr, nullptr};
@@ -221,6 +222,43 @@ static cudaError_t launch_msc_slab_queue(const MscHalf& p, const SlabOffset& so,
                       (long long)a0 * p.nw, total, per_warp, shift);
 }
 
+// Unmeasured msc half-sweep of a slab on the strip schedule of msc_strip_kernel (rows holding
+// whole 32-word strips): warp g walks rows a0 + band (g / strips) .. of strip g % strips, two
+// rows per step, with global Philox word indices and the slab's halo rows.
+constexpr int kSlabStripWarps = 8;
+
+__global__ void __launch_bounds__(kSlabStripWarps * 32, 2)
+    msc_slab_strip_kernel(const MscHalf p, const SlabOffset so, int a0, int an, int strips,
+                          int band)
+{
+    __shared__ StripSlots q_all[kSlabStripWarps];
+    __shared__ uint4 lvmask[16];
+    if (threadIdx.x < 16) lvmask[threadIdx.x] = level_masks(p.thr4, p.thr8, threadIdx.x);
+    pdl_wait();
+    pdl_trigger();
+    __syncthreads();
+    const int g = blockIdx.x * kSlabStripWarps + (threadIdx.x >> 5);
+    const int y0 = a0 + (g / strips) * band;
+    const int y1 = min(y0 + band, a0 + an);
+    if (y0 < a0 + an)
+        msc_strip_band<4, true>(p, g % strips, y0, y1, q_all[threadIdx.x >> 5], lvmask, so);
+}
+
+// Rows a0 .. a0 + an - 1 on the strip schedule, bands sized for one wave of resident warps.
+static cudaError_t launch_msc_slab_strip(const MscHalf& p, const SlabOffset& so, int a0, int an,
+                                         int sm_count, int blocks_per_sm, cudaStream_t st)
+{
+    const int strips = p.nw / 32;
+    const long long units = (long long)an * strips;
+    const long long warps = (long long)sm_count * blocks_per_sm * kSlabStripWarps;
+    long long band = (units + warps - 1) / warps;
+    if (band < 1) band = 1;
+    const long long nwarps = (long long)strips * ((an + band - 1) / band);
+    const unsigned blocks = (unsigned)((nwarps + kSlabStripWarps - 1) / kSlabStripWarps);
+    return launch_pdl(msc_slab_strip_kernel, dim3(blocks), dim3(kSlabStripWarps * 32), st, p, so,
+                      a0, an, strips, (int)band);
+}
+
 // The device seeded start of ising_fill_philox at global site indices.
 __global__ void slab_philox_int8_kernel(int8_t* c0, int8_t* c1, long long rows, long long row0,
                                         int lh, int pitch, u32 k0, u32 k1)
@@ -303,12 +341,16 @@ static int slab_half(ising_slab* s, int color, u32 t, int rule, unsigned long lo
         p.meas = meas;
         p.nw_magic = magic_for(s->nw);
         if (rule != kObserve && !meas) {
-            const cudaError_t e = launch_msc_slab_queue(
-                p,
-                SlabOffset{s->row0 * s->nw, (int)(s->begin & 1),
-                           reinterpret_cast<const u64*>(s->low_rows(1 - color)),
-                           reinterpret_cast<const u64*>(s->high_rows(1 - color))},
-                a0, an, s->sm_count, s->queue_blocks, s->stream);
+            const SlabOffset so{s->row0 * s->nw, (int)(s->begin & 1),
+                                reinterpret_cast<const u64*>(s->low_rows(1 - color)),
+                                reinterpret_cast<const u64*>(s->high_rows(1 - color))};
+            // strips where the rows hold whole 32-word strips (as for whole lattices)
+            const bool strips = s->nw % 32 == 0 && s->rows * s->nw <= 0xFFFFFFFFll;
+            const cudaError_t e =
+                strips ? launch_msc_slab_strip(p, so, a0, an, s->sm_count, s->strip_blocks,
+                                               s->stream)
+                       : launch_msc_slab_queue(p, so, a0, an, s->sm_count, s->queue_blocks,
+                                               s->stream);
             return e == cudaSuccess ? ISING_OK : cuda_fail(e, "slab half-sweep launch");
         }
         const unsigned grid = slab_grid((long long)an * s->nw, s->max_blocks);
@@ -448,6 +490,12 @@ int ising_slab_create(int ndim, const int64_t* shape, int variant, int algorithm
                                                           kSlabQueueWarps * 32, 0) == cudaSuccess &&
             b > 0)
             s->queue_blocks = b;
+        cudaGetLastError();
+        b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, msc_slab_strip_kernel,
+                                                          kSlabStripWarps * 32, 0) == cudaSuccess &&
+            b > 0)
+            s->strip_blocks = b;
         cudaGetLastError();
     }
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);

@@ -276,6 +276,8 @@ GPU_CASES = [
     ("int8", (12, 10, 40), "metropolis", 0.22, 3),
     ("int8", (10, 8, 32), "heatbath", 0.25, 4),
     ("msc", (34, 256), "metropolis", 0.44, 3),
+    ("msc", (38, 4096), "metropolis", 0.44, 3),  # 32-word rows: the strip schedule, odd slabs
+    ("msc", (20, 8192), "metropolis", 0.3, 2),
     ("int8", (32, 64), "heatbath", -0.3, 2),  # negative beta: the per-site lookup rule
 ]
 
