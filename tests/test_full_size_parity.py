@@ -10,6 +10,8 @@ thread.  All results are integers, so every comparison is exact.
   arrays and (M, E); plus the series every 100 sweeps.
 * int8 3D heat bath 256^3, beta 0.221654626, cold start, 2000 sweeps with (M, E) every 10: the
   200-point series and the final lattice.
+* int8 2D at 16384^2 (Metropolis), 8192^2 (heat bath) and 4096 x 4104 (rows padded to 16
+  bytes): the (M, E) series every 10 sweeps and the final colour arrays.
 * The 96-lattice ensemble (L = 2^k, k ~ U{6..12}, T ~ U[2.0, 2.6], seed = index, hot starts,
   5000 sweeps, (M, E) every 10) through the batched engine: every member's 500-point series
   and final lattice (the oracle's vectorised int8 half-sweep keeps its 1.4e12 updates to
@@ -88,3 +90,24 @@ def test_ensemble_of_96_lattices_against_the_oracle(oracle_mod):
         np.testing.assert_array_equal(res.series, ref.sweep(5000, measure_every=10),
                                       err_msg=f"L={job.shape[0]} seed={job.seed}")
         np.testing.assert_array_equal(res.lattice, ref.get_lattice())
+
+
+@pytest.mark.parametrize("shape,algorithm,beta,sweeps", [
+    ((16384, 16384), "metropolis", BETA_C_2D, 60),   # the band schedule's longest bands
+    ((8192, 8192), "heatbath", 0.42, 60),
+    ((4096, 4104), "metropolis", 0.4, 100),          # rows padded to 16 bytes (2052 sites)
+], ids=str)
+def test_int8_2d_large_lattices(oracle_mod, shape, algorithm, beta, sweeps):
+    """The plain int8 2D kernels on lattices of the served stream's largest sizes and the
+    headline's, hot start, against the oracle: the (M, E) series every 10 sweeps and the final
+    colour arrays."""
+    from pyising_b200.backend import B200Int8
+
+    lat = oracle_mod.random_lattice(shape, 5)
+    sim = B200Int8(shape, beta, seed=2**36 + 11, algorithm=algorithm, init=lat)
+    ref = oracle_mod.OracleInt8(shape, beta, seed=2**36 + 11, algorithm=algorithm, init=lat)
+    np.testing.assert_array_equal(sim.sweep_measured(sweeps, 10),
+                                  ref.sweep(sweeps, measure_every=10))
+    c0, c1 = sim.colour_arrays()
+    np.testing.assert_array_equal(c0, ref.c[0])
+    np.testing.assert_array_equal(c1, ref.c[1])
