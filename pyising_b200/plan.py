@@ -49,7 +49,7 @@ SPEC_BANDWIDTH_GBS = 7700.0  # B200 (HGX) HBM3e
 ROOT = Path(__file__).resolve().parent.parent
 # ncu summaries (profiles/<kernel>_<workload>.md) that match a plan row
 PROFILES = {("int8", 2, 16384, "metropolis"): "int8_half_kernel_int8_16384.md",
-            ("msc", 2, 16384, "metropolis"): "msc_half_queue_kernel_msc16384.md",
+            ("msc", 2, 16384, "metropolis"): "msc_strip_kernel_msc16384.md",
             ("int8", 3, 256, "heatbath"): "int8_half_kernel_int8_3d_256_heatbath.md"}
 
 
