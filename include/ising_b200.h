@@ -153,9 +153,6 @@ int ising_set_schedule(ising_sim* h, int schedule, int test_mute_band);
  * rows per step, with (Philox blocks per word before the work stack, resident blocks of 256
  * threads the registers are bounded for) = (4, 2), (4, 3), (4, 4), (3, 2), (3, 3), (3, 4). */
 #define ISING_KNOB_MSC_KERNEL 9
-/* int8 temporal tiles (schedule "temporal"): column tiles per row (0 = automatic: 128-byte
- * tiles where rows are 256 bytes or wider, 1 = whole rows, else 2, 4 or 8 tiles). */
-#define ISING_KNOB_TEMPORAL_COLS 11
 /* Test hook of the bounded union-find loops (0 = off): 1 makes every cluster labeling write a
  * two-site cycle into the labels (sites 0 and S) after the unions, so the root walks that follow
  * run out of their step budgets and the call returns ISING_ERR_TIMEOUT, with the context intact.

@@ -13,8 +13,7 @@ by site, sweep and colour, and every schedule visits the same sites with the sam
 * ``msc_waves``     msc: warps per resident warp (ranges or strip bands of the work-stack kernels);
 * ``graph_chunk``   sweeps per captured CUDA graph of an unmeasured run;
 * ``schedule``      ``"auto"`` (graphs), ``"launches"``, ``"persistent"`` or ``"temporal"``
-                    (2D int8: two sweeps per launch on shared-memory tiles);
-* ``temporal_cols`` column tiles per row of the temporal schedule (0 = automatic).
+                    (2D int8: two sweeps per launch on shared-memory tiles).
 
 :func:`tune` measures them on a scratch lattice of the given shape (device seeded start, CUDA
 events on the simulation's stream) by coordinate descent from the defaults, and stores the best
@@ -41,9 +40,9 @@ from . import _lib
 from ._lib import check, lib
 
 KNOBS = {"band": 1, "chunk_width": 2, "blocks_per_sm": 3, "msc_waves": 4, "graph_chunk": 5,
-         "msc_kernel": 9, "temporal_cols": 11}
+         "msc_kernel": 9}
 DEFAULTS = {"band": 0, "chunk_width": 16, "blocks_per_sm": 8, "msc_waves": 1, "graph_chunk": 32,
-            "msc_kernel": 0, "temporal_cols": 0, "schedule": "auto"}
+            "msc_kernel": 0, "schedule": "auto"}
 
 _lock = threading.Lock()
 _cache_mem: dict[Path, dict] = {}  # cache file contents by path, read once per process
@@ -89,7 +88,6 @@ def search_space(variant: str, shape, algorithm: str = "metropolis") -> dict[str
         space["schedule"] = ["auto", "launches", "persistent"]
         if lh % 16 == 0 and shape[0] % 8 == 0 and shape[0] >= 16 and 32 * lh <= 96 * 1024:
             space["schedule"].append("temporal")
-            space["temporal_cols"] = [0, 1] + [c for c in (2, 4, 8) if lh % (16 * c) == 0]
     else:
         space["schedule"] = ["auto", "launches"]
     space["graph_chunk"] = [32, 8, 128]

@@ -618,11 +618,6 @@ int ising_set_knob(ising_sim* h, int knob, int value)
         if (value < 0 || value > 7) return fail(ISING_ERR_INVALID, "msc kernel must be 0..7");
         h->msc_kernel = value;
         break;
-    case ISING_KNOB_TEMPORAL_COLS:
-        if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8)
-            return fail(ISING_ERR_INVALID, "temporal column tiles must be 0, 1, 2, 4 or 8");
-        h->temporal_cols = value;
-        break;
     case ISING_KNOB_TEST_LABEL_CYCLE:
         if (value != 0 && value != 1) return fail(ISING_ERR_INVALID, "test hook is 0 or 1");
         h->test_label_cycle = value;
@@ -645,7 +640,6 @@ int ising_get_knob(ising_sim* h, int knob, int* value)
     case ISING_KNOB_GRAPH_CHUNK: *value = (int)h->graph_chunk; break;
     case ISING_KNOB_CLUSTER_TILE: *value = h->cluster_tile; break;
     case ISING_KNOB_MSC_KERNEL: *value = h->msc_kernel; break;
-    case ISING_KNOB_TEMPORAL_COLS: *value = h->temporal_cols; break;
     case ISING_KNOB_TEST_LABEL_CYCLE: *value = h->test_label_cycle; break;
     default: return fail(ISING_ERR_INVALID, "unknown knob %d", knob);
     }

@@ -40,7 +40,6 @@ struct ising_sim {
     int blocks_per_sm = 8;
     int msc_waves = 1;                  // msc: warp ranges per resident warp
     int msc_kernel = 0;                 // msc: schedule (ISING_KNOB_MSC_KERNEL)
-    int temporal_cols = 0;              // int8 temporal tiles: column tiles per row (knob)
     int64_t graph_chunk = 32;           // sweeps per captured graph of an unmeasured run
     // Captured chunks of `sweeps` sweeps (one measurement at the end when `measured`), replayed
     // with the sweep counter and series slot in d_acc[6], d_acc[7].

@@ -136,93 +136,6 @@ __global__ void __launch_bounds__(kTbThreads) int8_temporal_kernel(const Int8Hal
     }
 }
 
-// Column tiles: the same four half-sweeps on a tile of kTbRows rows and one column range of
-// `tw` bytes (lh / tiles_per_row) plus one 16-byte chunk of halo on each side, so a band is
-// spread over several small CTAs and a few of them share an SM: while one waits at a step
-// barrier, the others issue.  Horizontally a half-sweep reads one site further out, so after
-// kTbSteps (<= 16) half-sweeps only the outer bytes of the halo chunks can be wrong (their
-// outermost neighbour lies outside the tile and is read as any byte of the tile): every halo
-// chunk is updated like the others, and only the inner columns of the band are written back.
-constexpr int kTbColThreads = 256;
-
-template <int RULE>
-__global__ void __launch_bounds__(kTbColThreads) int8_temporal_cols_kernel(const Int8Half p_in,
-                                                                           int8_t* c0, int8_t* c1,
-                                                                           int tw)
-{
-    constexpr int V = 16;
-    static_assert(kTbSteps <= 16, "halo chunks of 16 bytes");
-    extern __shared__ __align__(16) int8_t tile[];  // [colour][kTbRows][tw + 32]
-    __shared__ u32 stab[8];
-    Int8Half p = p_in;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int i = 0; i < 7; ++i) stab[i] = p.table[i];
-    }
-    pdl_wait();  // the previous launch of the stream has completed
-    pdl_trigger();
-    resolve_ctl(p);
-    const int lh = p.lh, ly = p.ly;
-    const int tiles = lh / tw;
-    const int band = blockIdx.x / tiles, col = blockIdx.x - band * tiles;
-    const int r0 = band * kTbBand;
-    const int sw = tw + 32, nch = sw / 16;  // tile width in bytes and chunks
-    const int jlo = col * tw - 16;         // global column of tile column 0 (mod lh)
-    for (int i = threadIdx.x; i < 2 * kTbRows * nch; i += blockDim.x) {
-        const int c = i >= kTbRows * nch;
-        const int rem = i - c * kTbRows * nch;
-        const int tr = rem / nch, jc = rem - tr * nch;
-        int gr = r0 - kTbSteps + tr;
-        gr = gr < 0 ? gr + ly : (gr >= ly ? gr - ly : gr);
-        int gj = jlo + 16 * jc;
-        gj = gj < 0 ? gj + lh : (gj >= lh ? gj - lh : gj);
-        *reinterpret_cast<uint4*>(tile + (c * kTbRows + tr) * sw + 16 * jc) =
-            __ldcg(reinterpret_cast<const uint4*>((c ? c1 : c0) + (long long)gr * p.pitch + gj));
-    }
-    __syncthreads();
-    long long m_acc = 0, e_acc = 0;  // unused (no measurement here)
-#pragma unroll 1
-    for (int k = 0; k < kTbSteps; ++k) {
-        const int color = k & 1;
-        Int8Half q = p;
-        q.t = p.t + (u32)(k >> 1);
-        q.color = (u32)color;
-        int8_t* own = tile + color * kTbRows * sw;
-        const int8_t* oth = tile + (color ^ 1) * kTbRows * sw;
-        const int lo = k + 1, n = (kTbRows - 2 - 2 * k) * nch;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int tr = lo + i / nch, jc = i - (i / nch) * nch, tj = 16 * jc;
-            int gr = r0 - kTbSteps + tr;
-            gr = gr < 0 ? gr + ly : (gr >= ly ? gr - ly : gr);
-            int gj = jlo + tj;
-            gj = gj < 0 ? gj + lh : (gj >= lh ? gj - lh : gj);
-            const int par = (gr + color) & 1;
-            const Words<V / 4> s = lds_words<V>(own + tr * sw + tj);
-            const Words<V / 4> c = lds_words<V>(oth + tr * sw + tj);
-            const Words<V / 4> nu = lds_words<V>(oth + (tr + 1) * sw + tj);
-            const Words<V / 4> nd = lds_words<V>(oth + (tr - 1) * sw + tj);
-            // the neighbour byte beyond the chunk; at the tile's edges any byte of the row
-            const int te = par ? (tj + V < sw ? tj + V : tj) : (tj > 0 ? tj - 1 : 0);
-            const u32 edge = (u32)(uint8_t)oth[tr * sw + te];
-            const Words<V / 4> ns = int8_update<V, 2, RULE, false, false, false>(
-                q, gr, par, gj, V / 4, s, c, nu, nd, nu, nd, edge, stab, m_acc, e_acc);
-            sts_words<V>(own + tr * sw + tj, ns);
-        }
-        __syncthreads();
-    }
-    // the band's rows, inner columns only
-    const int inner = tw / 16;
-    for (int i = threadIdx.x; i < 2 * kTbBand * inner; i += blockDim.x) {
-        const int c = i >= kTbBand * inner;
-        const int rem = i - c * kTbBand * inner;
-        const int b = rem / inner, jc = rem - b * inner;
-        *reinterpret_cast<uint4*>((c ? c1 : c0) + (long long)(r0 + b) * p.pitch + col * tw +
-                                  16 * jc) =
-            *reinterpret_cast<const uint4*>(tile + (c * kTbRows + kTbSteps + b) * sw +
-                                            16 * (jc + 1));
-    }
-}
-
 bool temporal_ok(const ising_sim* h)
 {
     return h->variant == ISING_VARIANT_INT8 && h->ndim == 2 &&
@@ -274,26 +187,6 @@ cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long 
         cfg.numAttrs = 1;
         return cudaLaunchKernelEx(&cfg, kernel, p, c0, c1);
     };
-    // column tiles of tw bytes (automatic: 128 bytes where the row is 256 or more bytes wide)
-    int tw = h->lh;
-    if (h->temporal_cols > 1) tw = h->lh / h->temporal_cols;
-    else if (h->temporal_cols == 0 && h->lh >= 256 && h->lh % 128 == 0) tw = 128;
-    if (tw < h->lh && tw % 16 == 0 && h->lh % tw == 0) {
-        const size_t csmem = (size_t)2 * kTbRows * (tw + 32);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(h->ly / kTbBand * (h->lh / tw)));
-        cfg.blockDim = dim3(kTbColThreads);
-        cfg.dynamicSmemBytes = csmem;
-        cfg.stream = h->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return h->rule == kHeatFast
-                   ? cudaLaunchKernelEx(&cfg, int8_temporal_cols_kernel<kHeatFast>, p, c0, c1, tw)
-                   : cudaLaunchKernelEx(&cfg, int8_temporal_cols_kernel<kMetroFast>, p, c0, c1, tw);
-    }
     return h->rule == kHeatFast ? launch(int8_temporal_kernel<kHeatFast>)
                                 : launch(int8_temporal_kernel<kMetroFast>);
 }

@@ -41,28 +41,6 @@ def test_schedules_match_oracle(oracle_mod, shape, algorithm, beta):
         np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice(), err_msg=schedule)
 
 
-@pytest.mark.parametrize("shape,algorithm,beta", [
-    ((32, 1024), "heatbath", 0.42),
-    ((48, 512), "metropolis", BETA_C_2D),
-], ids=str)
-@pytest.mark.parametrize("cols", [0, 1, 2, 4, 8])
-def test_temporal_column_tiles_match_oracle(oracle_mod, shape, algorithm, beta, cols):
-    """Temporal tiles split into column tiles (16-byte halo chunks on each side, updated like
-    the rest): every split gives the oracle's spins and series."""
-    from pyising_b200._lib import check, lib
-    from pyising_b200.backend import B200Int8
-
-    lat = oracle_mod.random_lattice(shape, 4)
-    ref = oracle_mod.OracleInt8(shape, beta, seed=2**34 + 3, algorithm=algorithm, init=lat)
-    sim = B200Int8(shape, beta, seed=2**34 + 3, algorithm=algorithm, init=lat)
-    sim.set_schedule("temporal")
-    check(lib().ising_set_knob(sim._h, 11, cols), "set_knob")  # ISING_KNOB_TEMPORAL_COLS
-    sim.sweep(38)
-    ref.sweep(38)
-    np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice())
-    np.testing.assert_array_equal(sim.sweep_measured(20, 5), ref.sweep(20, measure_every=5))
-
-
 def test_temporal_c1_golden():
     """C1 on the temporally blocked schedule (two sweeps per launch between measurements)."""
     from pyising_b200.backend import B200Int8
