@@ -198,13 +198,14 @@ static int chunk_graph(ising_sim* h, int64_t G, bool measured, cudaGraphExec_t* 
     int rc = ISING_OK;
     const bool tb = use_temporal(h);
     const int K = temporal_sweeps();
-    for (int64_t s = 0; s < G && rc == ISING_OK;) {
-        if (tb && s + K <= G - (measured ? 1 : 0)) {  // K unmeasured sweeps in one launch
-            const cudaError_t le = launch_int8_temporal(h, (u32)s, ctl);
-            if (le != cudaSuccess) rc = cuda_fail(le, "temporal half-sweeps");
-            s += K;
-            continue;
-        }
+    int64_t s = 0;
+    if (tb) {  // K unmeasured sweeps per launch, up to the measured last sweep
+        const int64_t runs = (G - (measured ? 1 : 0)) / K;
+        const cudaError_t le = launch_temporal_run(h, 0u, runs, ctl);
+        if (le != cudaSuccess) rc = cuda_fail(le, "temporal half-sweeps");
+        s = runs * K;
+    }
+    for (; s < G && rc == ISING_OK;) {
         unsigned long long* m =
             (measured && s == G - 1) ? (unsigned long long*)h->d_series : nullptr;
         rc = half_sweep(h, 0, (u32)s, nullptr, nullptr, ctl);
@@ -383,6 +384,8 @@ int ising_destroy(ising_sim* h)
         if (h->c[c]) cudaFreeAsync(h->c[c], fs);
     if (h->d_acc) cudaFreeAsync(h->d_acc, fs);
     if (h->d_series) cudaFreeAsync(h->d_series, fs);
+    for (int c = 0; c < 2; ++c)
+        if (h->tb_scratch[c]) cudaFreeAsync(h->tb_scratch[c], fs);
     if (h->h_series) host_pinned_put(h->h_series, (size_t)h->series_cap * 2 * sizeof(long long));
     if (fs) cudaStreamSynchronize(fs);
     clear_graphs(h);
@@ -695,6 +698,10 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
         TRY_CUDA(cudaMemsetAsync(h->d_series, 0, (size_t)n_meas * 2 * sizeof(long long),
                                  h->stream));
     }
+    if (use_temporal(h)) {  // before any graph capture
+        int rc = temporal_scratch(h);
+        if (rc != ISING_OK) return rc;
+    }
     int64_t k = 0, s0 = 0;
     // Small 2D int8 lattices: all sweeps in one persistent cooperative launch.
     const bool persistent_ok = h->variant == ISING_VARIANT_INT8 && h->ndim == 2 &&
@@ -766,8 +773,10 @@ int ising_sweep(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_eve
         const u32 t = (u32)(t0 + (uint64_t)s);
         const bool meas = measure_every > 0 && (s + 1) % measure_every == 0;
         if (tb && s + K <= n_sweeps && unmeasured(s)) {
-            TRY_CUDA(launch_int8_temporal(h, t, nullptr));  // sweeps s .. s + K - 1
-            s += K - 1;
+            int64_t runs = 0;  // consecutive launches of K unmeasured sweeps from s
+            while (s + (runs + 1) * K <= n_sweeps && unmeasured(s + runs * K)) ++runs;
+            TRY_CUDA(launch_temporal_run(h, t, runs, nullptr));
+            s += runs * K - 1;
             continue;
         }
         unsigned long long* m = meas ? (unsigned long long*)(h->d_series + 2 * k) : nullptr;

@@ -54,6 +54,7 @@ struct ising_sim {
     unsigned int* d_flags = nullptr;    // persistent schedule: per-band progress + error word
     int* d_label = nullptr;             // cluster updates: a label per site, error word, masks
     int cluster_tile = 0;               // cluster updates: positions per tile (0: automatic)
+    void* tb_scratch[2] = {nullptr, nullptr};  // temporal schedule: second pair of colour arrays
     int test_label_cycle = 0;           // test hook: a cycle in the cluster labels
     bool pending_err = false;           // a persistent run's error word not yet read
 };
@@ -72,7 +73,14 @@ int half_sweep(ising_sim* h, int color, u32 t, unsigned long long* meas,
 void clear_graphs(ising_sim* h);
 int observe(ising_sim* h, unsigned long long* acc);
 bool temporal_ok(const ising_sim* h);
-cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long long* ctl);
+// Stream-ordered device memory from the per-device pool that single-lattice handles share.
+cudaError_t pool_alloc(int device, void** p, size_t bytes, cudaStream_t st);
+// The temporal schedule's second pair of colour arrays (allocated once, outside any capture).
+int temporal_scratch(ising_sim* h);
+// `count` temporal launches of kTbSteps / 2 sweeps each from sweep t; the lattice ends in the
+// handle's arrays.
+cudaError_t launch_temporal_run(const ising_sim* h, u32 t, int64_t count,
+                                const unsigned long long* ctl);
 int temporal_sweeps();  // sweeps per temporal launch
 int run_persistent_int8(ising_sim* h, uint64_t t0, int64_t n_sweeps, int64_t measure_every,
                         unsigned long long* series, unsigned int* flags, int* err, int mute_band);

@@ -70,9 +70,12 @@ __device__ __forceinline__ void sts_words(int8_t* p, const Words<V / 4>& w)
     else *reinterpret_cast<u32*>(p) = w.v[0];
 }
 
+// Reads both colours from in0/in1 and writes the band to out0/out1: separate arrays, since a
+// CTA's halo rows are other CTAs' bands, which those write back in the same launch.
 template <int RULE>
-__global__ void __launch_bounds__(kTbThreads) int8_temporal_kernel(const Int8Half p_in, int8_t* c0,
-                                                           int8_t* c1)
+__global__ void __launch_bounds__(kTbThreads) int8_temporal_kernel(const Int8Half p_in,
+                                                           const int8_t* in0, const int8_t* in1,
+                                                           int8_t* out0, int8_t* out1)
 {
     constexpr int V = kTbChunk;
     extern __shared__ __align__(16) int8_t tile[];  // [colour][kTbRows][lh]
@@ -94,7 +97,7 @@ __global__ void __launch_bounds__(kTbThreads) int8_temporal_kernel(const Int8Hal
         const int tr = rem / cpr, jc = rem - tr * cpr;
         int gr = r0 - kTbSteps + tr;
         gr = gr < 0 ? gr + ly : (gr >= ly ? gr - ly : gr);
-        const int8_t* src = (c ? c1 : c0) + (long long)gr * p.pitch + 16 * jc;
+        const int8_t* src = (c ? in1 : in0) + (long long)gr * p.pitch + 16 * jc;
         *reinterpret_cast<uint4*>(tile + (c * kTbRows + tr) * lh + 16 * jc) =
             __ldcg(reinterpret_cast<const uint4*>(src));
     }
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(kTbThreads) int8_temporal_kernel(const Int8Hal
         const int c = i >= kTbBand * cpr;
         const int rem = i - c * kTbBand * cpr;
         const int b = rem / cpr, jc = rem - b * cpr;
-        *reinterpret_cast<uint4*>((c ? c1 : c0) + (long long)(r0 + b) * p.pitch + 16 * jc) =
+        *reinterpret_cast<uint4*>((c ? out1 : out0) + (long long)(r0 + b) * p.pitch + 16 * jc) =
             *reinterpret_cast<const uint4*>(tile + (c * kTbRows + kTbSteps + b) * lh + 16 * jc);
     }
 }
@@ -146,8 +149,10 @@ bool temporal_ok(const ising_sim* h)
 
 int temporal_sweeps() { return kTbSteps / 2; }
 
-// kTbSteps / 2 sweeps from sweep t (relative to ctl[0] when ctl is set), colour 0 first.
-cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long long* ctl)
+// kTbSteps / 2 sweeps from sweep t (relative to ctl[0] when ctl is set), colour 0 first,
+// from the handle's arrays into its scratch pair (to_scratch) or back.
+static cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long long* ctl,
+                                        bool to_scratch)
 {
     Int8Half p;
     memset(&p, 0, sizeof p);
@@ -167,8 +172,14 @@ cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long 
     p.ctl = ctl;
     const size_t smem = (size_t)2 * kTbRows * h->lh;
     const dim3 grid((unsigned)(h->ly / kTbBand)), block(kTbThreads);
-    int8_t* c0 = (int8_t*)h->c[0];
-    int8_t* c1 = (int8_t*)h->c[1];
+    int8_t* a0 = (int8_t*)h->c[0];
+    int8_t* a1 = (int8_t*)h->c[1];
+    int8_t* b0 = (int8_t*)h->tb_scratch[0];
+    int8_t* b1 = (int8_t*)h->tb_scratch[1];
+    const int8_t* i0 = to_scratch ? a0 : b0;
+    const int8_t* i1 = to_scratch ? a1 : b1;
+    int8_t* o0 = to_scratch ? b0 : a0;
+    int8_t* o1 = to_scratch ? b1 : a1;
     auto launch = [&](auto kernel) -> cudaError_t {
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -185,10 +196,44 @@ cudaError_t launch_int8_temporal(const ising_sim* h, u32 t, const unsigned long 
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, kernel, p, c0, c1);
+        return cudaLaunchKernelEx(&cfg, kernel, p, i0, i1, o0, o1);
     };
     return h->rule == kHeatFast ? launch(int8_temporal_kernel<kHeatFast>)
                                 : launch(int8_temporal_kernel<kMetroFast>);
+}
+
+int temporal_scratch(ising_sim* h)
+{
+    for (int c = 0; c < 2; ++c) {
+        if (h->tb_scratch[c]) continue;
+        const cudaError_t e = pool_alloc(h->device, &h->tb_scratch[c], h->colour_bytes, h->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            h->tb_scratch[c] = nullptr;
+            return fail(ISING_ERR_NOMEM, "allocation of the temporal schedule's second arrays");
+        }
+    }
+    return ISING_OK;
+}
+
+// `count` temporal launches from sweep t (each kTbSteps / 2 sweeps), alternating between the
+// handle's arrays and the scratch pair; an odd count ends with the lattice copied back.
+cudaError_t launch_temporal_run(const ising_sim* h, u32 t, int64_t count,
+                                const unsigned long long* ctl)
+{
+    const u32 K = (u32)(kTbSteps / 2);
+    for (int64_t i = 0; i < count; ++i) {
+        const cudaError_t e = launch_int8_temporal(h, t + (u32)i * K, ctl, (i & 1) == 0);
+        if (e != cudaSuccess) return e;
+    }
+    if (count & 1) {
+        for (int c = 0; c < 2; ++c) {
+            const cudaError_t e = cudaMemcpyAsync(h->c[c], h->tb_scratch[c], h->colour_bytes,
+                                                  cudaMemcpyDeviceToDevice, h->stream);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 }  // namespace ising

@@ -41,6 +41,28 @@ def test_schedules_match_oracle(oracle_mod, shape, algorithm, beta):
         np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice(), err_msg=schedule)
 
 
+@pytest.mark.parametrize("shape,algorithm,beta", [
+    ((2048, 2048), "metropolis", BETA_C_2D),  # 256 bands: more CTAs than one wave holds
+    ((2400, 256), "heatbath", 0.42),
+], ids=str)
+def test_temporal_tiles_read_and_write_separate_arrays(oracle_mod, shape, algorithm, beta):
+    """A temporal launch reads one pair of colour arrays and writes the other (a CTA's halo rows
+    are other CTAs' bands, rewritten in the same launch): with more bands than resident CTAs,
+    and with odd and even numbers of launches between measurements, the oracle's results."""
+    from pyising_b200.backend import B200Int8
+
+    lat = oracle_mod.random_lattice(shape, 8)
+    ref = oracle_mod.OracleInt8(shape, beta, seed=2**33 + 1, algorithm=algorithm, init=lat)
+    sim = B200Int8(shape, beta, seed=2**33 + 1, algorithm=algorithm, init=lat)
+    sim.set_schedule("temporal")
+    for n in (6, 8, 2, 3):  # 3, 4, 1 launches and one launch plus a single sweep
+        sim.sweep(n)
+        ref.sweep(n)
+        np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice(), err_msg=str(n))
+    np.testing.assert_array_equal(sim.sweep_measured(21, 7), ref.sweep(21, measure_every=7))
+    np.testing.assert_array_equal(sim.get_lattice(), ref.get_lattice())
+
+
 def test_temporal_c1_golden():
     """C1 on the temporally blocked schedule (two sweeps per launch between measurements)."""
     from pyising_b200.backend import B200Int8
