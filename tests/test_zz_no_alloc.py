@@ -25,6 +25,7 @@ CASES = [
     ("int8", (16, 24), "heatbath", 0.42),
     ("int8", (16, 16, 32), "heatbath", 0.22),
     ("msc", (128, 256), "metropolis", 0.44),
+    ("msc", (40, 4096), "metropolis", 0.44),  # rows of 32 words: the strip kernel
 ]
 
 
