@@ -13,7 +13,9 @@ pytestmark = pytest.mark.gpu
 KNOB_MSC_KERNEL = 9
 
 
-@pytest.mark.parametrize("shape", [(64, 4096), (34, 8192), (16, 12288), (128, 1024)], ids=str)
+# (4800, 4096): bands of 3 rows, so the two-row steps and a final single row both run
+@pytest.mark.parametrize("shape", [(64, 4096), (34, 8192), (16, 12288), (128, 1024),
+                                   (4800, 4096)], ids=str)
 @pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_msc_schedules_match_the_oracle(oracle_mod, shape, kernel):
     from pyising_b200._lib import check, lib
