@@ -108,8 +108,10 @@ __device__ __forceinline__ void msc_word(const MscHalf& p, int y, int x, long lo
 //     batch was consumed) are bit-sliced and get four Philox blocks each unconditionally (at
 //     T_c half of the words need four or more); decided words are stored, the others pushed on
 //     the warp's 64-entry stack in shared memory;
-//   * while the stack holds 32 or more entries (or the range is done): pop up to 32, draw one
-//     Philox block each at the entry's own level pair, store finished words, push back the rest.
+//   * while the stack holds 32 or more entries: pop 32, draw one Philox block each at the
+//     entry's own level pair, store finished words, push back the rest;
+//   * when the range is done and at most 32 entries are left: each lane runs one entry to the
+//     end (stack_drain).
 // The random numbers, bit levels and their order are the reference's; only the schedule
 // differs, so results are identical.  Lanes are handled as two independent 32-bit halves.
 
@@ -153,6 +155,26 @@ __device__ __forceinline__ void call_levels(const u32x4& r, const uint4& m, u32 
     level32(r.y, m.x, m.y, a1h, undh, resh);
     level32(r.z, m.z, m.w, a1l, undl, resl);  // odd level: r2 | r3 << 32
     level32(r.w, m.z, m.w, a1h, undh, resh);
+}
+
+// Both levels of one Philox block on 32 lanes: the even level uses r_e, the odd one r_o.
+__device__ __forceinline__ void level_pair(u32 re, u32 ro, u32 t4e, u32 t8e, u32 t4o, u32 t8o,
+                                           u32 a1, u32& und, u32& acc)
+{
+    const u32 tme = (a1 & t4e) | (~a1 & t8e);
+    const u32 tmo = (a1 & t4o) | (~a1 & t8o);
+    const u32 ae = und & ~re & tme;       // decided at the even level, accepted
+    const u32 u1 = und & ~(re ^ tme);     // still undecided after it
+    const u32 ao = u1 & ~ro & tmo;
+    und = u1 & ~(ro ^ tmo);
+    acc |= ae | ao;
+}
+
+__device__ __forceinline__ void block_levels(const u32x4& r, const uint4& m, u32 a1l, u32 a1h,
+                                             u32& undl, u32& undh, u32& accl, u32& acch)
+{
+    level_pair(r.x, r.z, m.x, m.y, m.z, m.w, a1l, undl, accl);  // r0 | r1 << 32, r2 | r3 << 32
+    level_pair(r.y, r.w, m.x, m.y, m.z, m.w, a1h, undh, acch);
 }
 
 // Where a lattice piece sits in a bigger lattice (slab decomposition): the Philox word index is
@@ -204,6 +226,44 @@ __device__ __forceinline__ void intake_load(const MscHalf& p, long long w, bool 
         L.up = __ldg(p.other + (long long)(y == 0 ? p.rows - 1 : y - 1) * nw + x);
         L.dn = __ldg(p.other + (long long)(y + 1 == p.rows ? 0 : y + 1) * nw + x);
     }
+}
+
+// The end of a warp's work: the at most 32 stack entries left take one lane each, and each lane
+// draws its entry's Philox blocks one after another until the entry is decided, without going
+// back to the stack.  Draining by stack passes instead (pop, one block, push back the undecided)
+// spends a pop, a ballot and a push per block on a warp whose lanes are mostly idle; here the
+// passes' bookkeeping is gone and only the lanes' longest chain remains (measured on B200 with
+// the strip walker: 16384^2 3546 -> 3647 flips/ns, 8192^2 2535 -> 2790, 4096^2 1387 -> 1716;
+// drawing two or more of an entry's blocks at a time was no faster).  Works on both stack
+// layouts (QueueSlots, StripSlots).
+template <class Slots>
+__device__ __forceinline__ void stack_drain(const MscHalf& p, Slots& q, int& n,
+                                            const uint4* lvmask, u32 wg)
+{
+    const int lane = threadIdx.x & 31;
+    const bool act = lane < n;
+    u32 idx = 0, lp = 0, undl = 0, undh = 0, accl = 0, acch = 0;
+    u64 a1 = 0, res = 0;
+    if (act) {
+        idx = q.idx[lane];
+        lp = q.lp[lane];
+        a1 = q.a1[lane];
+        res = q.res[lane];
+        const u64 und = q.und[lane];
+        undl = (u32)und;
+        undh = (u32)(und >> 32);
+    }
+    __syncwarp();
+    n = 0;
+    if (act) {
+        const u32 a1l = (u32)a1, a1h = (u32)(a1 >> 32);
+        do {  // an entry has lp < 16 and an undecided lane
+            const u32x4 r = philox4x32_10<true>(wg + idx, p.t, p.color, 1u + lp, p.k0, p.k1);
+            block_levels(r, lvmask[lp], a1l, a1h, undl, undh, accl, acch);
+        } while ((undl | undh) != 0 && ++lp < 16u);
+        p.own[idx] = res ^ ((u64)accl | ((u64)acch << 32));
+    }
+    __syncwarp();
 }
 
 // The whole warp updates words [begin, end) of the lattice in p.  `lvmask` holds
@@ -266,7 +326,10 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             }
             n += __popc(km);
             __syncwarp();
-        } else if (n > 0) {
+        } else if (!more && n <= 32) {
+            if (n > 0) stack_drain(p, q, n, lvmask, wg);
+            break;
+        } else {
             // pop up to kPop entries: lane l takes entries base + l and base + 32 + l
             const int take = n < kPop ? n : kPop;
             const int base = n - take;
@@ -316,8 +379,6 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             }
             n = base + kept;
             __syncwarp();
-        } else {
-            break;
         }
     }
 }
@@ -349,26 +410,6 @@ __device__ __forceinline__ HalfSlices slice_half(u32 o, u32 n1, u32 n2, u32 n3, 
     h.a1 = (s1 ^ s2) & ~cc;
     h.a2 = cc | (s1 & s2);
     return h;
-}
-
-// Both levels of one Philox block on 32 lanes: the even level uses r_e, the odd one r_o.
-__device__ __forceinline__ void level_pair(u32 re, u32 ro, u32 t4e, u32 t8e, u32 t4o, u32 t8o,
-                                           u32 a1, u32& und, u32& acc)
-{
-    const u32 tme = (a1 & t4e) | (~a1 & t8e);
-    const u32 tmo = (a1 & t4o) | (~a1 & t8o);
-    const u32 ae = und & ~re & tme;       // decided at the even level, accepted
-    const u32 u1 = und & ~(re ^ tme);     // still undecided after it
-    const u32 ao = u1 & ~ro & tmo;
-    und = u1 & ~(ro ^ tmo);
-    acc |= ae | ao;
-}
-
-__device__ __forceinline__ void block_levels(const u32x4& r, const uint4& m, u32 a1l, u32 a1h,
-                                             u32& undl, u32& undh, u32& accl, u32& acch)
-{
-    level_pair(r.x, r.z, m.x, m.y, m.z, m.w, a1l, undl, accl);  // r0 | r1 << 32, r2 | r3 << 32
-    level_pair(r.y, r.w, m.x, m.y, m.z, m.w, a1h, undh, acch);
 }
 
 // The warp walks its band two rows per step: each lane takes word x of rows y and y + 1, so
@@ -526,10 +567,11 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             }
             n += __popc(kmb);
             __syncwarp();
-        } else if (n > 0) {
-            strip_pop(p, q, n, lvmask, wg);
-        } else {
+        } else if (y >= y1 && n <= 32) {
+            if (n > 0) stack_drain(p, q, n, lvmask, wg);
             break;
+        } else {
+            strip_pop(p, q, n, lvmask, wg);
         }
     }
 }
