@@ -253,15 +253,16 @@ def tune_ensemble(jobs, sweeps: int = 200, device: int = 0) -> dict:
     from .ensemble import Ensemble
 
     short = [dataclasses.replace(j, sweeps=min(j.sweeps, sweeps)) for j in jobs]
-    flips = sum(j.n_spins * j.sweeps for j in short)
 
     def run(cfg: dict) -> float:
         with Ensemble(device=device) as ens:
             for name, v in cfg.items():
                 ens.set_knob(name, v)
-            for j in short:
-                ens.add(j)
+            ids = [ens.add(j) for j in short]
             ens.run(2)  # admission, first work list and module loading outside the timing
+            # the flips still to do: the first sweep (two epochs) already ran
+            flips = sum(j.n_spins * (j.sweeps - ens.status(i)[1])
+                        for j, i in zip(short, ids, strict=True))
             t0 = time.perf_counter()
             ens.run()
             dt = time.perf_counter() - t0

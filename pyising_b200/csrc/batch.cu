@@ -369,7 +369,9 @@ public:
     int64_t used_bytes() const { return used_; }
 
     // One half-sweep of every active lattice (admitting pending jobs at even epochs).
-    int step()
+    // Issues the next epoch, or the next replayed chunk of 2 * chunk_sweeps_ epochs when the
+    // batch is stable and `budget` (epochs the caller still allows; <= 0: no limit) holds it.
+    int step(long long budget = 0)
     {
         cudaError_t e = cudaSetDevice(device_);
         if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
@@ -384,7 +386,7 @@ public:
             if (rc != ISING_OK) return rc;
         }
         reap_chunks();
-        if (chunk_ready()) {
+        if (chunk_ready() && (budget <= 0 || 2 * chunk_sweeps_ <= budget)) {
             int rc = run_chunk();
             if (rc == ISING_OK) rc = retire();
             if (rc == ISING_OK) rc = throttle();
@@ -1172,13 +1174,14 @@ int ising_batch_add(ising_batch* b, const ising_job* job, int64_t* id)
 int ising_batch_run(ising_batch* b, int64_t max_epochs, int64_t* epochs_run)
 {
     if (!b) return fail(ISING_ERR_INVALID, "null batch");
-    int64_t n = 0;
+    int64_t n = 0;  // half-sweep epochs issued (a replayed chunk issues many)
     while (b->eng->has_work() && (max_epochs <= 0 || n < max_epochs)) {
         const size_t before = b->eng->active_count() + b->eng->pending_count();
-        int rc = b->eng->step();
+        const long long e0 = b->eng->epoch();
+        int rc = b->eng->step(max_epochs > 0 ? max_epochs - n : 0);
         if (rc == ISING_OK) rc = b->eng->wait_throttle();
         if (rc != ISING_OK) return rc;
-        ++n;
+        n += b->eng->epoch() - e0;
         if (b->eng->active_count() == 0 && b->eng->pending_count() > 0 &&
             b->eng->pending_count() == before)
             return fail(ISING_ERR_NOMEM, "pending jobs do not fit the memory budget");

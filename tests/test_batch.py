@@ -93,6 +93,32 @@ def test_ensemble_members_equal_solo_runs(oracle_mod):
             ens.release(jid)
 
 
+def test_run_counts_half_sweeps_with_graph_chunks(oracle_mod):
+    """run(k) advances exactly k half-sweeps, also while the batch replays graph chunks of many
+    sweeps (a chunk that does not fit the k left is not replayed), and a run split into pieces
+    gives the results of the job alone."""
+    from pyising_b200.ensemble import Ensemble, Job
+
+    jobs = [Job((64, 64), BETA_C_2D, 120, seed=s, measure_every=10, keep_lattice=True)
+            for s in range(3)]
+    with Ensemble(memory_budget=1 << 30) as ens:
+        ens.set_knob("graph_chunk", 8)
+        ids = [ens.add(j) for j in jobs]
+        assert ens.run(2) == 2
+        assert all(ens.status(i) == ("active", 1) for i in ids)
+        assert ens.run(37) == 37  # ends between the two colours of a sweep
+        assert all(ens.status(i) == ("active", 19) for i in ids)
+        assert ens.run(70) == 70
+        assert all(ens.status(i) == ("active", 54) for i in ids)
+        ens.run()
+        for jid, job in zip(ids, jobs, strict=True):
+            assert ens.status(jid) == ("done", job.sweeps)
+            want_series, want_lat = solo(job, oracle_mod)
+            res = ens.result(jid)
+            np.testing.assert_array_equal(res.series, want_series)
+            np.testing.assert_array_equal(res.lattice, want_lat)
+
+
 def test_ensemble_small_budget_admits_in_turns(oracle_mod):
     """A budget that holds about two lattices at a time: jobs wait and join at later sweep
     boundaries, and the results are unchanged."""
