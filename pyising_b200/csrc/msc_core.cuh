@@ -122,12 +122,14 @@ constexpr int kPop = 32 * ISING_MSC_POP;  // entries popped per pass (two per la
 constexpr int kQueueCap = kPop + 32;
 constexpr int kIntakeCalls = ISING_MSC_INTAKE_CALLS;  // Philox blocks per word before queueing
 
+// One more slot than entries: lanes with nothing to push write to slot kQueueCap, so a push is
+// stores without a branch.
 struct QueueSlots {
-    u32 idx[kQueueCap];
-    u32 lp[kQueueCap];
-    u64 a1[kQueueCap];
-    u64 und[kQueueCap];
-    u64 res[kQueueCap];
+    u32 idx[kQueueCap + 1];
+    u32 lp[kQueueCap + 1];
+    u64 a1[kQueueCap + 1];
+    u64 und[kQueueCap + 1];
+    u64 res[kQueueCap + 1];
 };
 
 // Threshold bit masks of the even and odd level of each level pair: (t4e, t8e, t4o, t8o).
@@ -316,8 +318,8 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
             const bool keep = valid && (undl | undh) != 0;
             if (valid && !keep) p.own[wc] = (u64)resl | ((u64)resh << 32);
             const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
-            if (keep) {
-                const int pos = n + __popc(km & lt);
+            {
+                const int pos = keep ? n + __popc(km & lt) : kQueueCap;
                 q.idx[pos] = (u32)wc;
                 q.lp[pos] = (u32)kIntakeCalls;
                 q.a1[pos] = (u64)a1l | ((u64)a1h << 32);
@@ -367,8 +369,8 @@ __device__ __forceinline__ void msc_queue_range(const MscHalf& p, long long begi
                 const bool keep = act[m] && (undl[m] | undh[m]) != 0 && lp[m] < 16u;
                 if (act[m] && !keep) p.own[idx[m]] = (u64)resl[m] | ((u64)resh[m] << 32);
                 const u32 km = __ballot_sync(0xFFFFFFFFu, keep);
-                if (keep) {
-                    const int pos = base + kept + __popc(km & lt);
+                {
+                    const int pos = keep ? base + kept + __popc(km & lt) : kQueueCap;
                     q.idx[pos] = idx[m];
                     q.lp[pos] = lp[m];
                     q.a1[pos] = a1[m];
@@ -421,12 +423,15 @@ __device__ __forceinline__ HalfSlices slice_half(u32 o, u32 n1, u32 n2, u32 n3, 
 // in uniform registers).
 constexpr int kStripCap = kPop + 64;
 
+// One more slot than entries: lanes with nothing to push write their entry to slot kStripCap,
+// so a push is stores without a branch (measured 1.2% faster than the per-lane branch, in the
+// word-range walker too).
 struct StripSlots {
-    u32 idx[kStripCap];
-    u32 lp[kStripCap];
-    u64 a1[kStripCap];
-    u64 und[kStripCap];
-    u64 res[kStripCap];
+    u32 idx[kStripCap + 1];
+    u32 lp[kStripCap + 1];
+    u64 a1[kStripCap + 1];
+    u64 und[kStripCap + 1];
+    u64 res[kStripCap + 1];
 };
 
 // One pass over the stack: a Philox block for each of up to 32 entries at its own level pair;
@@ -552,8 +557,8 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
             if (two) p.own[wb] = (u64)rbl | ((u64)rbh << 32);
             const u32 kma = __ballot_sync(0xFFFFFFFFu, ka);
             const u32 kmb = __ballot_sync(0xFFFFFFFFu, kb);
-            if (ka) {
-                const int pos = n + __popc(kma & lt);
+            {
+                const int pos = ka ? n + __popc(kma & lt) : kStripCap;
                 q.idx[pos] = wa;
                 q.lp[pos] = (u32)K;
                 q.a1[pos] = (u64)al.a1 | ((u64)ah.a1 << 32);
@@ -561,8 +566,8 @@ __device__ __forceinline__ void msc_strip_band(const MscHalf& p, int strip, int 
                 q.res[pos] = (u64)ral | ((u64)rah << 32);
             }
             n += __popc(kma);
-            if (kb) {
-                const int pos = n + __popc(kmb & lt);
+            {
+                const int pos = kb ? n + __popc(kmb & lt) : kStripCap;
                 q.idx[pos] = wb;
                 q.lp[pos] = (u32)K;
                 q.a1[pos] = (u64)bl.a1 | ((u64)bh.a1 << 32);
